@@ -1,0 +1,324 @@
+"""Benchmark: slice-propagations/s (forward + adjoint) of the batched MSET
+hot path on the mid-size synthetic tilt series.
+
+Workload ("mid"): 128^3 FP32 volume at 0.3 A/voxel from a seeded fcc
+Cu/Au-like lattice of Gaussian atoms, 128^2 complex64 window, 32x32 scan at
+3 px, 21 tilts over +-60 deg, 64 slices of 2 voxels: 21,504 positions and
+1,376,256 slice-propagations per step.  One step = one batched pass: forward
+(transmission, 64 x [FFT, propagator, IFFT]), far field, residual, loss and the
+adjoint with V / probe / scan-position gradients of every position of every
+tilt, in one persistent launch.  Inputs (measured amplitudes 1.4 GB) exceed
+L2, so no flush is needed between steps.
+
+One JSON line on stdout (rank 0).  --impl reference times the FP64 CPU port
+of the reference's path (the reference's own CPU path is MATLAB code, which
+is not available here) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def flops_per_unit(n: int) -> float:
+    """FFTW convention: 4 FFTs of n x n (5 N^2 log2 N^2 each) + 32 N^2 pointwise."""
+    n2 = n * n
+    return 4 * 5 * n2 * math.log2(n2) + 32 * n2
+
+
+def flops_per_position(n: int) -> float:
+    n2 = n * n
+    return 6 * 5 * n2 * math.log2(n2) + 40 * n2
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# ---------------------------------------------------------------------------
+def build_problem(cfg_name: str, rank: int, device: int, method: int = 1, adjoint: int = 0):
+    import torch
+
+    from mset_b200 import synth
+    from mset_b200.batch import BatchSession
+
+    cfg = synth.CONFIGS[cfg_name]
+    cfg = synth.Config(**{**cfg.__dict__, "seed": cfg.seed + 7919 * rank})
+    spec = synth.make_specimen(cfg)
+    npos = [spec.scan_x.size] * cfg.n_tilts
+    bs = BatchSession(n=cfg.window, nz=cfg.vol[0], npos=npos, prop=spec.prop, sigma=spec.sigma,
+                      potential_pixelsize=cfg.dx, slice_binning=cfg.slice_binning, method=method,
+                      adjoint=adjoint, device=device)
+    # simulate the measured intensities with the library's own forward model
+    for j, v in enumerate(spec.volumes):
+        bs.set_tilt(j, probe=spec.probe, scan_x=spec.scan_x, scan_y=spec.scan_y,
+                    measured=np.zeros((npos[j], cfg.window, cfg.window), np.float32), volume=v)
+    inten = bs.simulate()
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(cfg.seed + 1000)
+    it = torch.from_numpy(inten).to(f"cuda:{device}")
+    meas = torch.poisson(it.clamp_min(0), generator=g).cpu().numpy().astype(np.float32)
+    del it, inten
+    # reconstruction state: half the true potential (a mid-iteration estimate)
+    off = 0
+    for j, v in enumerate(spec.volumes):
+        bs.set_tilt(j, measured=meas[off:off + npos[j]], volume=0.5 * v)
+        off += npos[j]
+    return cfg, spec, bs, meas
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    cfg, spec, bs, meas = build_problem(args.config, rank, local)
+    n = cfg.window
+    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    positions = int(bs.npos.sum())
+    units = positions * ns
+
+    # warm-up (untimed)
+    for _ in range(max(args.warmup, 0)):
+        bs.gradient(want=())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    if rank == 0:
+        sampler.start()
+    ms = bs.time_gradient(args.steps)  # CUDA events on the session stream, K passes
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if rank == 0 else {}
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * units / (ms / 1e3)
+
+    # end to end through the C ABI with host buffers: volumes in, gradients out
+    vols = [np.ascontiguousarray(0.5 * v) for v in spec.volumes]
+    grad = np.zeros((cfg.n_tilts, ns, n, n))
+    err = np.zeros(cfg.n_tilts)
+    import ctypes as C
+    from mset_b200._lib import check, dptr, fptr
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for j in range(cfg.n_tilts):
+            check("mset_batch_set_volume", bs._lib.mset_batch_set_volume(bs._h, j, fptr(vols[j])))
+        check("mset_batch_gradient", bs._lib.mset_batch_gradient(bs._h, dptr(grad), None, None, dptr(err)))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+
+    if rank == 0:
+        peaks = measured_peaks()
+        sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+        fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, FMA counted as 2
+        flop = units * flops_per_unit(n) + positions * flops_per_position(n)
+        achieved = flop / (ms / 1e3) / 1e12
+        cpu = cpu_baseline(args, cfg, spec, meas) if not args.no_cpu else None
+        line = {
+            "metric": "slice-propagations/s (fwd+adjoint)",
+            "value": value,
+            "unit": "slice-propagations/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "s_per_step": ms / 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "fp32 (complex64 propagation, fp64 reductions)",
+            "data": "synthetic (seeded fcc Cu/Au-like Gaussian-atom lattice, Poisson 1e4 e-/probe)",
+            "config": {"workload": "mid: 128^3 volume, 128^2 window, 32x32 scan, 21 tilts, 64 slabs x 2 voxels, "
+                                   "batched gradient pass over all 21504 positions",
+                       "positions_per_gpu": positions, "slabs": ns, "window": n,
+                       "units_per_step_per_gpu": units, "l2": "inputs larger than L2 (1.4 GB amplitudes)",
+                       "parallelism": f"tilt replicas x{world}"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": None,
+                         "peak_source": f"nominal FP32 CUDA-core peak 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz "
+                                        "(MEASURED_PEAKS has no FP32 figure)",
+                         "flop_per_unit": flops_per_unit(n), "flop_per_position": flops_per_position(n)},
+            "e2e": {"value": world * units / e2e_s, "unit": "slice-propagations/s",
+                    "h2d_bytes_per_step": int(sum(v.nbytes for v in vols)),
+                    "d2h_bytes_per_step": int(grad.nbytes + err.nbytes)},
+            "gpu_launches": args.steps * bs._lib.mset_batch_launch_count(bs._h),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    bs.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_sample_positions(cores: int) -> int:
+    return int(max(8, min(96, 6 * cores)))
+
+
+def cpu_baseline(args, cfg, spec, meas) -> dict:
+    """FP64 CPU port (oracle) on a bounded sample of the same workload."""
+    from oracle import oracle as O
+
+    cores = O.max_threads()
+    k = cpu_sample_positions(cores)
+    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    t0 = time.perf_counter()
+    O.batched_tilt(0.5 * spec.volumes[0], spec.probe, spec.prop, spec.scan_x[:k], spec.scan_y[:k], meas[:k],
+                   sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
+            "sample": f"{k} positions of tilt 0 of the same workload (FP64 C port of the reference path, "
+                      f"OpenMP over positions), {dt:.1f} s"}
+
+
+def run_reference(args):
+    """The reference arm: the FP64 CPU port of the reference's path on the
+    host cores, on a bounded sample of the same workload per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from mset_b200 import synth
+    from oracle import oracle as O
+    from tests.helpers import small_case  # noqa: F401
+
+    cfg = synth.CONFIGS[args.config]
+    spec = synth.make_specimen(cfg, with_volumes=False)
+    rng = np.random.default_rng(cfg.seed)
+    pos, peak = synth.atoms(cfg, rng)
+    v = synth.pad_lateral(synth.voxelise(pos, peak, cfg.vol, cfg.dx, cfg.blob_sigma), cfg.window).astype(np.float32)
+    cores = O.max_threads()
+    k = max(4, cpu_sample_positions(cores) // 4)
+    n = cfg.window
+    meas = np.full((k, n, n), 1.0, np.float32)
+    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    for _ in range(max(args.warmup, 0) and 1):
+        O.batched_tilt(0.5 * v, spec.probe, spec.prop, spec.scan_x[:1], spec.scan_y[:1], meas[:1],
+                       sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.batched_tilt(0.5 * v, spec.probe, spec.prop, spec.scan_x[:k], spec.scan_y[:k], meas, sigma=spec.sigma,
+                       dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = k * ns / dt
+    line = {
+        "impl": "reference",
+        "metric": "slice-propagations/s (fwd+adjoint)",
+        "value": value,
+        "unit": "slice-propagations/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dt * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp64",
+        "data": "synthetic",
+        "config": {"workload": "mid: 128^3 volume, 128^2 window, 32x32 scan, 21 tilts, 64 slabs x 2 voxels "
+                               f"(sampled: {k} positions per step)"},
+        "cpu_baseline": {"value": value, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} positions x {ns} slabs per step; the reference's own CPU path is MATLAB "
+                                   "code (STEP02/STEP03), unavailable on this box, so its FP64 C port is timed"},
+        "e2e": {"value": value, "unit": "slice-propagations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="mid")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * mset_b200.h -- C ABI of the B200-native MSET multislice hot path.
+ *
+ * The MEX-compatible entry points keep the argument layout of the reference's
+ * CUDA MEX module (jhlee0667/MSET, src/CUDA/mex_main.cu), so a caller that
+ * drives `mset_cuda_kernel('upload' | 'run_mset' | 'run_sset' | 'error_mset' |
+ * 'error_sset', STEM_data, measured_cells)` can call these instead:
+ *
+ *   reference mode string                     replacement
+ *   'upload'     (mex_main.cu:42-95)          mset_upload / mset_mex_upload
+ *   'run_mset'   (mex_main.cu:27-28, 98-155)  mset_run(mode = MSET_MODE_MSET)
+ *   'run_sset'   (mex_main.cu:29-30, 98-155)  mset_run(mode = MSET_MODE_SSET)
+ *   'error_mset' (mex_main.cu:31-32,157-184)  mset_error(mode = MSET_MODE_MSET)
+ *   'error_sset' (mex_main.cu:33-34,157-184)  mset_error(mode = MSET_MODE_SSET)
+ *   clear mset_cuda_kernel (Run_MSET_recon.m:174)   mset_destroy / mset_mex_clear
+ *
+ * Array layouts are the MEX ones: MATLAB column-major arrays seen as C arrays
+ * with the dimensions reversed (mex_tools.hpp:15-24):
+ *   RVol         float [nz][n][n]            (MATLAB size n x n x nz)
+ *   init_wave2D  float [n][n][2]             complex interleaved (re, im)
+ *   prop2D       float [n][n][2]             centred propagator (the library ifftshifts it)
+ *   measured     float [num_scan_pos][n][n]  one pattern per position, centred
+ *                (cell element k = position k, mset.cu:201)
+ *   scan_xlist / scan_ylist  float [num_scan_pos], 1-based pixels; x pairs with
+ *                the fastest (MATLAB dim-1) axis.
+ * All pointers in this header are HOST pointers unless a name ends in _dev.
+ *
+ * Every function returns 0 on success or a negative MSET_E* status; it never
+ * aborts.  mset_last_error() gives the message of the calling thread's last
+ * failure.  A session is not thread-safe; different sessions are independent.
+ */
+#ifndef MSET_B200_H
+#define MSET_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSET_MODE_MSET 1 /* multislice (run_main_mset, mset.cu:80-334) */
+#define MSET_MODE_SSET 2 /* single slice (run_main_sset, mset.cu:345-546) */
+
+#define MSET_ADJOINT_REF 0   /* reference V-gradient: conj of the wave saved after the slab (mset.cu:248-251) */
+#define MSET_ADJOINT_EXACT 1 /* exact adjoint: conj of the wave entering the slab, spectral position derivative */
+
+#define MSET_OK 0
+#define MSET_E_ARG -1         /* invalid argument (null pointer, bad size, bad mode) */
+#define MSET_E_UNSUPPORTED -2 /* window size without a compiled kernel, non-square window */
+#define MSET_E_CUDA -3        /* CUDA runtime error (message in mset_last_error) */
+#define MSET_E_STATE -4       /* call out of order (e.g. run before upload) */
+#define MSET_E_NOMEM -5       /* device allocation failed */
+
+typedef struct mset_session mset_session;
+
+/* Scalars and arrays of the STEM_data struct fields read by the MEX upload
+ * (mex_main.cu:59-75; field names kept). */
+typedef struct {
+    int32_t n;                 /* lateral size: RVol is n x n x nz (square, mset.cu:83) */
+    int32_t nz;                /* depth */
+    int32_t num_scan_pos;
+    int32_t N_scan_x, N_scan_y;
+    float sigma;               /* interaction constant, rad/(V*Angstrom) */
+    float potential_pixelsize; /* Angstrom per voxel (slice thickness dz) */
+    float alpha, E0;           /* accepted and ignored, as in the reference */
+    float step_size[3];        /* object, probe, scan-position step sizes */
+    int32_t slice_binning;
+    const float *RVol;
+    const float *init_wave2D;
+    const float *prop2D;
+    const float *scan_xlist;
+    const float *scan_ylist;
+    const float *measured;
+} mset_upload_args;
+
+/* ---- session lifetime ---------------------------------------------------- */
+int mset_create(int device, mset_session **out);
+int mset_destroy(mset_session *s);
+const char *mset_last_error(void);
+/* version string of the library */
+const char *mset_version(void);
+
+/* ---- MEX-compatible entry points ------------------------------------------ */
+/* 'upload' (mex_main.cu:42-95): copy the struct fields and the measured
+ * patterns to the device, zero the error accumulator.  Device buffers are kept
+ * and reused when the next upload has the same sizes. */
+int mset_upload(mset_session *s, const mset_upload_args *a);
+/* 'run_mset' / 'run_sset' (mex_main.cu:98-155): one sequential pass over all
+ * positions with the reference's per-position updates of RVol, probe and scan
+ * positions.  Outputs (host, caller-allocated): rvol_out [nz][n][n],
+ * probe_out [n][n][2], scan_x_out / scan_y_out [num_scan_pos]; error_out may be
+ * NULL (the MEX's nlhs == 4) or receives the accumulated error normalised as
+ * mex_main.cu:150. */
+int mset_run(mset_session *s, int mode, float *rvol_out, float *probe_out, float *scan_x_out,
+             float *scan_y_out, float *error_out);
+/* same as mset_run with the adjoint formula selectable (MSET_ADJOINT_*) */
+int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *probe_out,
+                float *scan_x_out, float *scan_y_out, float *error_out);
+/* 'error_mset' / 'error_sset' (mex_main.cu:157-184): forward pass over all
+ * positions, error accumulated and normalised as mex_main.cu:179. */
+int mset_error(mset_session *s, int mode, float *error_out);
+
+/* global-session shims with the MEX's lifetime (one implicit session per
+ * process, recreated by every upload, mex_main.cu:13, 56) */
+int mset_mex_upload(const mset_upload_args *a);
+int mset_mex_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out,
+                 float *error_out);
+int mset_mex_error(int mode, float *error_out);
+int mset_mex_clear(void);
+
+/* ---- batched method --------------------------------------------------------
+ * Every position of every tilt sees the same volume, probe and positions; the
+ * gradients of all positions are accumulated in FP64 in one persistent launch.
+ * Tilt j has its own beam-frame volume V_j, probe, scan positions and measured
+ * patterns, all resident on the device. */
+typedef struct {
+    int32_t n, nz, slice_binning;
+    int32_t method;  /* MSET_MODE_* */
+    int32_t adjoint; /* MSET_ADJOINT_* */
+    float sigma, potential_pixelsize;
+    float step_size[3];
+    int32_t ntilts;
+    const int32_t *npos; /* [ntilts] positions per tilt */
+    const float *prop2D; /* [n][n][2] centred propagator */
+} mset_batch_args;
+
+int mset_batch_setup(mset_session *s, const mset_batch_args *a);
+/* tilt j: probe [n][n][2], scan_x/scan_y [npos_j], measured [npos_j][n][n]
+ * (centred), volume [nz][n][n] in the tilt's beam frame (NULL keeps the
+ * current one). */
+int mset_batch_set_tilt(mset_session *s, int j, const float *probe, const float *scan_x,
+                        const float *scan_y, const float *measured, const float *volume);
+int mset_batch_set_volume(mset_session *s, int j, const float *volume);
+/* one batched pass: forward + adjoint of every position of every tilt.
+ * Outputs (host, any may be NULL: results then stay on the device):
+ *   grad_out   [ntilts][ns][n][n] double: sum over positions of Re(g) per slab
+ *   probe_out  [ntilts][n][n][2] double: sum over positions of F^{-1}(chi0) fs(-s),
+ *              standard FFT order; its forward FFT is sum_p shift_{-s_p}(chi0_p),
+ *              the probe direction of mset.cu:288-309 summed over positions
+ *   posdir_out [sum npos][2] double: scan-position directions
+ *   err_out    [ntilts] double: sum over positions and pixels of (A - M)^2 */
+int mset_batch_gradient(mset_session *s, double *grad_out, double *probe_out, double *posdir_out,
+                        double *err_out);
+/* forward-only pass: err_out [ntilts] as above */
+int mset_batch_error(mset_session *s, double *err_out);
+/* forward-only pass writing |Psi|^2 (centred layout) of every position:
+ * inten_out [sum npos][n][n] */
+int mset_batch_simulate(mset_session *s, float *inten_out);
+/* apply the last batched gradient: V_j += step0 * G_j, probe_j -= step1 * P_j,
+ * positions += step2 * posdir */
+int mset_batch_apply(mset_session *s);
+/* read back tilt j's state: volume [nz][n][n], probe [n][n][2], scan_x/y [npos_j] */
+int mset_batch_get_tilt(mset_session *s, int j, float *volume, float *probe, float *scan_x, float *scan_y);
+/* device-side timing helpers for benchmarks: run the batched gradient pass
+ * `reps` times on resident data and return the mean device time per pass in
+ * milliseconds measured with CUDA events on the session stream */
+int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
+/* number of kernel launches issued by one mset_batch_gradient call */
+int mset_batch_launch_count(mset_session *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSET_B200_H */

@@ -1,0 +1,110 @@
+"""Batched method: every position of every tilt in one persistent launch.
+
+All positions of all tilts see the same beam-frame volume, probe and scan
+positions; the gradients are accumulated in FP64 on the device
+(include/mset_b200.h, ``mset_batch_*``).  This changes the reference's
+sequential per-position update (src/CUDA/mset.cu:107-333) into a gradient
+step over the whole tilt series.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import MSET_ADJOINT_REF, MSET_MODE_MSET, check, dptr, fptr
+from .session import _c32, _cplx_f32
+
+
+class BatchSession:
+    def __init__(self, *, n: int, nz: int, npos: Sequence[int], prop, sigma: float,
+                 potential_pixelsize: float, slice_binning: int = 1, method: int = MSET_MODE_MSET,
+                 adjoint: int = MSET_ADJOINT_REF, step_size=(0.0, 0.0, 0.0), device: int = 0):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        check("mset_create", self._lib.mset_create(int(device), C.byref(h)))
+        self._h = h
+        self.n, self.nz = int(n), int(nz)
+        self.b = min(int(slice_binning), self.nz)
+        self.method = int(method)
+        self.ns = 1 if self.method == 2 else -(-self.nz // self.b)
+        self.npos = np.ascontiguousarray(np.asarray(npos, dtype=np.int32))
+        self.ntilts = int(self.npos.size)
+        self._prop = _cplx_f32(prop)
+        a = _lib.BatchArgs()
+        a.n, a.nz, a.slice_binning = self.n, self.nz, int(slice_binning)
+        a.method, a.adjoint = self.method, int(adjoint)
+        a.sigma, a.potential_pixelsize = float(sigma), float(potential_pixelsize)
+        a.step_size[:] = [float(v) for v in step_size]
+        a.ntilts = self.ntilts
+        a.npos = self.npos.ctypes.data_as(C.POINTER(C.c_int32))
+        a.prop2D = fptr(self._prop)
+        check("mset_batch_setup", self._lib.mset_batch_setup(self._h, C.byref(a)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tilt(self, j: int, *, probe=None, scan_x=None, scan_y=None, measured=None, volume=None):
+        pr = _cplx_f32(probe) if probe is not None else None
+        sx = _c32(scan_x).reshape(-1) if scan_x is not None else None
+        sy = _c32(scan_y).reshape(-1) if scan_y is not None else None
+        me = _c32(measured) if measured is not None else None
+        vo = _c32(volume) if volume is not None else None
+        check("mset_batch_set_tilt", self._lib.mset_batch_set_tilt(
+            self._h, int(j), fptr(pr), fptr(sx), fptr(sy), fptr(me), fptr(vo)))
+
+    def gradient(self, want=("grad", "probe", "posdir", "err")):
+        n2 = self.n * self.n
+        g = np.zeros((self.ntilts, self.ns, self.n, self.n)) if "grad" in want else None
+        p = np.zeros((self.ntilts, self.n, self.n, 2)) if "probe" in want else None
+        d = np.zeros((int(self.npos.sum()), 2)) if "posdir" in want else None
+        e = np.zeros(self.ntilts) if "err" in want else None
+        check("mset_batch_gradient", self._lib.mset_batch_gradient(self._h, dptr(g), dptr(p), dptr(d), dptr(e)))
+        out = {}
+        if g is not None:
+            out["grad"] = g
+        if p is not None:
+            out["probe"] = p[..., 0] + 1j * p[..., 1]
+        if d is not None:
+            out["posdir"] = d
+        if e is not None:
+            out["err"] = e
+        del n2
+        return out
+
+    def error(self) -> np.ndarray:
+        e = np.zeros(self.ntilts)
+        check("mset_batch_error", self._lib.mset_batch_error(self._h, dptr(e)))
+        return e
+
+    def simulate(self) -> np.ndarray:
+        out = np.empty((int(self.npos.sum()), self.n, self.n), np.float32)
+        check("mset_batch_simulate", self._lib.mset_batch_simulate(self._h, fptr(out)))
+        return out
+
+    def apply(self):
+        check("mset_batch_apply", self._lib.mset_batch_apply(self._h))
+
+    def get_tilt(self, j: int):
+        v = np.empty((self.nz, self.n, self.n), np.float32)
+        p = np.empty((self.n, self.n, 2), np.float32)
+        k = max(int(self.npos[j]), 1)
+        sx = np.empty(k, np.float32)
+        sy = np.empty(k, np.float32)
+        check("mset_batch_get_tilt", self._lib.mset_batch_get_tilt(self._h, int(j), fptr(v), fptr(p), fptr(sx), fptr(sy)))
+        return v, p.view(np.complex64).reshape(self.n, self.n), sx[: self.npos[j]], sy[: self.npos[j]]
+
+    def time_gradient(self, reps: int) -> float:
+        ms = np.zeros(1)
+        check("mset_batch_time", self._lib.mset_batch_time(self._h, int(reps), dptr(ms)))
+        return float(ms[0])

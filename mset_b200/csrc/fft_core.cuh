@@ -1,0 +1,347 @@
+// fft_core.cuh -- shared-memory 2D FFT building blocks for sm_100a.
+//
+// An N x N complex64 field lives in one CTA's shared memory, row stride
+// S = N + N/R1 (one pad element after every R1 elements along x, which makes
+// every pass below free of bank conflicts).  A 1D transform of length
+// N = R1*R2 is two register passes:
+//
+//   pass A (per n1, R2 points at x = n1 + R1*j):   R2-point DFT + twiddle
+//   pass B (per k2, R1 points at x = j + R1*k2):   R1-point DFT
+//
+// Natural -> scrambled (NAT2SCR): A then B.  Location L = k1 + R1*k2 then
+// holds frequency k = k2 + R2*k1 ("digit-reversed" order).
+// Scrambled -> natural (SCR2NAT): B then A (twiddle before the DFT).
+//
+// A forward transform, a pointwise product and an inverse transform therefore
+// need no reordering at all: the propagator, measured amplitudes and probe
+// spectrum are stored in the scrambled layout once, at upload.  Both
+// directions work with either sign, so the same passes give F and F^{-1}.
+//
+// The 2D transform is rows (x) then columns (y); the inverse runs columns then
+// rows.  The passes that border a pointwise stage are fused with it:
+//   row pass A  = [inverse rows A] + op(real space, natural order) + [forward rows A]
+//   col pass B  = [forward cols B] + op(Fourier space, scrambled)   + [inverse cols B]
+// so one propagation slab costs six shared-memory round trips.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mset {
+
+// ---------------------------------------------------------------------------
+// compile-time trigonometry (Taylor series in double, evaluated by the
+// compiler) for the internal twiddles of the register codelets
+// ---------------------------------------------------------------------------
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+constexpr double ct_reduce(double x) {
+    // x in [0, 2pi) -> [-pi, pi)
+    return x >= kPi ? x - 2.0 * kPi : x;
+}
+constexpr double ct_sin_series(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 30; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ct_cos_series(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 30; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+// e^{sign * 2 pi i m / r}
+template <int M, int R, int SG>
+struct Tw {
+    static constexpr double a = ct_reduce(2.0 * kPi * (double)(M % R) / (double)R);
+    static constexpr float c = (float)ct_cos_series(a);
+    static constexpr float s = (float)(SG * ct_sin_series(a));
+};
+
+template <int V>
+struct IC {
+    static constexpr int value = V;
+};
+template <int B, int E, class F>
+__device__ __forceinline__ void sfor(F &&f) {
+    if constexpr (B < E) {
+        f(IC<B>{});
+        sfor<B + 1, E>(f);
+    }
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by i * sg
+template <int SG>
+__device__ __forceinline__ float2 cmul_i(float2 a) {
+    return SG > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+template <int M, int R, int SG>
+__device__ __forceinline__ float2 twmul(float2 a) {
+    constexpr int m = M % R;
+    if constexpr (m == 0) {
+        return a;
+    } else if constexpr (4 * m == R) {
+        return cmul_i<SG>(a);
+    } else if constexpr (2 * m == R) {
+        return make_float2(-a.x, -a.y);
+    } else if constexpr (4 * m == 3 * R) {
+        return cmul_i<-SG>(a);
+    } else {
+        return cmul(a, make_float2(Tw<M, R, SG>::c, Tw<M, R, SG>::s));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// register DFT codelets: v[k] <- sum_j v[j] e^{SG 2 pi i jk/R}
+// ---------------------------------------------------------------------------
+template <int R, int SG>
+struct DFT;
+
+template <int SG>
+struct DFT<1, SG> {
+    static __device__ __forceinline__ void run(float2 *) {}
+};
+template <int SG>
+struct DFT<2, SG> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+template <int SG>
+struct DFT<3, SG> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        constexpr float c = -0.5f;
+        constexpr float s = (float)(SG * 0.86602540378443864676372317075294);
+        float2 a = v[0], b = v[1], d = v[2];
+        float2 t = cadd(b, d);
+        float2 u = csub(b, d);
+        float2 m = make_float2(fmaf(c, t.x, a.x), fmaf(c, t.y, a.y));
+        // i*s*u
+        float2 w = make_float2(-s * u.y, s * u.x);
+        v[0] = cadd(a, t);
+        v[1] = cadd(m, w);
+        v[2] = csub(m, w);
+    }
+};
+template <int SG>
+struct DFT<4, SG> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        float2 b0 = cadd(v[1], v[3]), b1 = cmul_i<SG>(csub(v[1], v[3]));
+        v[0] = cadd(a0, b0);
+        v[2] = csub(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[3] = csub(a1, b1);
+    }
+};
+template <int SG>
+struct DFT<5, SG> {
+    static __device__ __forceinline__ void run(float2 *v) {
+        constexpr float c1 = (float)0.30901699437494742410229341718282;   // cos(2pi/5)
+        constexpr float c2 = (float)-0.80901699437494742410229341718282;  // cos(4pi/5)
+        constexpr float s1 = (float)(SG * 0.95105651629515357211643933337938);
+        constexpr float s2 = (float)(SG * 0.58778525229247312916870595463907);
+        float2 x0 = v[0];
+        float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        float2 u1 = csub(v[1], v[4]), u2 = csub(v[2], v[3]);
+        float2 m1 = make_float2(x0.x + c1 * t1.x + c2 * t2.x, x0.y + c1 * t1.y + c2 * t2.y);
+        float2 m2 = make_float2(x0.x + c2 * t1.x + c1 * t2.x, x0.y + c2 * t1.y + c1 * t2.y);
+        // i*(s1 u1 + s2 u2), i*(s2 u1 - s1 u2)
+        float2 n1 = make_float2(s1 * u1.x + s2 * u2.x, s1 * u1.y + s2 * u2.y);
+        float2 n2 = make_float2(s2 * u1.x - s1 * u2.x, s2 * u1.y - s1 * u2.y);
+        v[0] = cadd(x0, cadd(t1, t2));
+        v[1] = make_float2(m1.x - n1.y, m1.y + n1.x);
+        v[4] = make_float2(m1.x + n1.y, m1.y - n1.x);
+        v[2] = make_float2(m2.x - n2.y, m2.y + n2.x);
+        v[3] = make_float2(m2.x + n2.y, m2.y - n2.x);
+    }
+};
+
+// composite sizes: R = P*Q, six-step in registers
+template <int R>
+struct Split {
+    static constexpr int P = (R % 4 == 0 && R > 4) ? 4 : (R % 2 == 0 ? 2 : (R % 3 == 0 ? 3 : 5));
+    static constexpr int Q = R / P;
+};
+template <int R, int SG>
+struct DFT {
+    static_assert(R == 6 || R == 8 || R == 10 || R == 12 || R == 16 || R == 9 || R == 15 || R == 20,
+                  "unsupported codelet size");
+    static __device__ __forceinline__ void run(float2 *v) {
+        constexpr int P = Split<R>::P, Q = Split<R>::Q;
+        float2 t[R];
+        sfor<0, P>([&](auto j1c) {
+            constexpr int j1 = decltype(j1c)::value;
+            float2 u[Q];
+            sfor<0, Q>([&](auto j2c) {
+                constexpr int j2 = decltype(j2c)::value;
+                u[j2] = v[j1 + P * j2];
+            });
+            DFT<Q, SG>::run(u);
+            sfor<0, Q>([&](auto k2c) {
+                constexpr int k2 = decltype(k2c)::value;
+                t[j1 * Q + k2] = twmul<j1 * k2, R, SG>(u[k2]);
+            });
+        });
+        sfor<0, Q>([&](auto k2c) {
+            constexpr int k2 = decltype(k2c)::value;
+            float2 w[P];
+            sfor<0, P>([&](auto j1c) {
+                constexpr int j1 = decltype(j1c)::value;
+                w[j1] = t[j1 * Q + k2];
+            });
+            DFT<P, SG>::run(w);
+            sfor<0, P>([&](auto k1c) {
+                constexpr int k1 = decltype(k1c)::value;
+                v[k2 + Q * k1] = w[k1];
+            });
+        });
+    }
+};
+
+// ---------------------------------------------------------------------------
+// geometry of one N x N field in shared memory
+// ---------------------------------------------------------------------------
+template <int N_, int R1_, int NT_, int MINB_ = 1>
+struct Geo {
+    static constexpr int MINB = MINB_;  // CTAs per SM the register budget is sized for
+    static constexpr int N = N_;
+    static constexpr int R1 = R1_;
+    static constexpr int R2 = N_ / R1_;
+    static constexpr int NT = NT_;
+    static constexpr int S = N + N / R1;  // padded row stride (elements)
+    static constexpr int NRA = N * R1;    // row/col pass-A tasks (R2 points each)
+    static constexpr int NRB = N * R2;    // row/col pass-B tasks (R1 points each)
+    static_assert(R1 * R2 == N, "N must equal R1*R2");
+    __device__ __forceinline__ static int px(int x) { return x + x / R1; }
+    __device__ __forceinline__ static int at(int y, int x) { return y * S + px(x); }
+    // scrambled location -> frequency index
+    __host__ __device__ __forceinline__ static int scr(int L) { return L / R1 + R2 * (L % R1); }
+};
+
+// twiddle W_N^{n1 k2} with sign (table holds e^{-2 pi i m/N} as [k2][n1])
+template <class G, int SG>
+__device__ __forceinline__ float2 twN(const float2 *tw, int n1, int k2) {
+    float2 w = tw[k2 * G::R1 + n1];
+    return SG < 0 ? w : cconj(w);
+}
+
+// Row pass A.  Task (y, n1) owns x = n1 + R1*j, j < R2.
+//   IN  != 0 : finish a scrambled->natural transform of sign IN
+//   op(y, n1, v) : pointwise stage on natural-order real-space values
+//   OUT != 0 : start a natural->scrambled transform of sign OUT
+template <class G, int IN, int OUT, class Op>
+__device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op) {
+    constexpr int R1 = G::R1, R2 = G::R2;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < G::NRA; t += G::NT) {
+        const int n1 = t % R1, y = t / R1;
+        float2 *row = buf + y * G::S + n1;
+        float2 v[R2];
+#pragma unroll
+        for (int j = 0; j < R2; ++j) v[j] = row[(R1 + 1) * j];
+        if constexpr (IN != 0) {
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, IN>(tw, n1, k2));
+            DFT<R2, IN>::run(v);
+        }
+        op(y, n1, v);
+        if constexpr (OUT != 0) {
+            DFT<R2, OUT>::run(v);
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, OUT>(tw, n1, k2));
+        }
+#pragma unroll
+        for (int j = 0; j < R2; ++j) row[(R1 + 1) * j] = v[j];
+    }
+}
+
+// Row pass B.  Task (y, k2) owns x = j + R1*k2, j < R1.
+template <class G, int SG>
+__device__ __forceinline__ void row_passB(float2 *buf) {
+    constexpr int R1 = G::R1, R2 = G::R2;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < G::NRB; t += G::NT) {
+        const int k2 = t % R2, y = t / R2;
+        float2 *p = buf + y * G::S + (R1 + 1) * k2;
+        float2 v[R1];
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = p[j];
+        DFT<R1, SG>::run(v);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) p[j] = v[j];
+    }
+}
+
+// Column pass A.  Task (x, n1) owns rows y = n1 + R1*j.
+//   FWD: natural->scrambled step (DFT then twiddle); else scrambled->natural
+template <class G, int SG, bool FWD>
+__device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
+    constexpr int R1 = G::R1, R2 = G::R2;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < G::NRA; t += G::NT) {
+        const int x = t % G::N, n1 = t / G::N;
+        float2 *p = buf + n1 * G::S + G::px(x);
+        float2 v[R2];
+#pragma unroll
+        for (int j = 0; j < R2; ++j) v[j] = p[R1 * G::S * j];
+        if constexpr (FWD) {
+            DFT<R2, SG>::run(v);
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+        } else {
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+            DFT<R2, SG>::run(v);
+        }
+#pragma unroll
+        for (int j = 0; j < R2; ++j) p[R1 * G::S * j] = v[j];
+    }
+}
+
+// Column pass B.  Task (x, k2) owns rows Ly = j + R1*k2 (scrambled).
+//   IN  != 0 : finish natural->scrambled (sign IN)
+//   op(Ly0, x, v) : pointwise stage on scrambled spectrum, element j at row Ly0 + j
+//   OUT != 0 : start scrambled->natural (sign OUT)
+template <class G, int IN, int OUT, class Op>
+__device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
+    constexpr int R1 = G::R1;
+#pragma unroll 1
+    for (int t = threadIdx.x; t < G::NRB; t += G::NT) {
+        const int x = t % G::N, k2 = t / G::N;
+        const int y0 = R1 * k2;
+        float2 *p = buf + y0 * G::S + G::px(x);
+        float2 v[R1];
+#pragma unroll
+        for (int j = 0; j < R1; ++j) v[j] = p[G::S * j];
+        if constexpr (IN != 0) DFT<R1, IN>::run(v);
+        op(y0, x, v);
+        if constexpr (OUT != 0) DFT<R1, OUT>::run(v);
+#pragma unroll
+        for (int j = 0; j < R1; ++j) p[G::S * j] = v[j];
+    }
+}
+
+struct NoOp {
+    template <class... A>
+    __device__ __forceinline__ void operator()(A &&...) const {}
+};
+
+}  // namespace mset

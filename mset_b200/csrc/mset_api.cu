@@ -1,0 +1,652 @@
+// mset_api.cu -- C ABI (include/mset_b200.h): sessions, validation, device
+// buffers, the MEX-compatible modes and the batched method.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mset_b200.h"
+#include "mset_kernels.cuh"
+
+using namespace mset;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char b[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b, sizeof b, fmt, ap);
+    va_end(ap);
+    g_err = b;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    return fail(MSET_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define CK(call)                                                    \
+    do {                                                            \
+        cudaError_t e_ = (call);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);         \
+    } while (0)
+
+#define CKL(rc, what)                                                                 \
+    do {                                                                              \
+        int rc_ = (rc);                                                               \
+        if (rc_ != 0) return cuda_fail((cudaError_t)rc_, what);                       \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // (re)allocate when the element count changes; contents undefined
+    cudaError_t ensure(size_t count) {
+        if (count == n && p) return cudaSuccess;
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc((void **)&p, sizeof(T) * count);
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+};
+
+}  // namespace
+
+struct TiltBufs {
+    DevBuf<float> V;
+    DevBuf<float2> Q;
+    DevBuf<float> amp;
+    DevBuf<float> sx, sy;
+    DevBuf<double> grad, qacc, posdir;
+    int npos = 0;
+};
+
+struct mset_session {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    int sms = 0;
+    // geometry
+    int n = 0, nz = 0, b = 1, ns = 0;
+    int method = kMSET, adjoint = kREF;
+    float sigma = 0, dz = 0, step[3] = {0, 0, 0};
+    int nsx = 0, nsy = 0;
+    Plan plan{};
+    bool ready = false;
+    bool batch = false;
+    // tilts (1 for the MEX-style session)
+    std::vector<TiltBufs> tilts;
+    std::vector<int> npos;
+    std::vector<int> pos_off;
+    int total_pos = 0;
+    // shared buffers
+    DevBuf<float2> pscr, twn, save, tmpc;
+    DevBuf<float> meas_tmp;
+    DevBuf<double> err;
+    DevBuf<TiltDev> d_tilts;
+    DevBuf<int2> items;
+    DevBuf<unsigned> counter;
+    DevBuf<float> inten;
+    int save_slots = 0;
+    std::vector<TiltDev> h_tilts;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int set_device(mset_session *s) {
+    CK(cudaSetDevice(s->device));
+    return 0;
+}
+
+// twiddle table e^{-2 pi i n1 k2 / N} stored as [k2][n1], computed in double
+int upload_twiddles(mset_session *s) {
+    const int n = s->plan.n, r1 = s->plan.r1, r2 = n / r1;
+    std::vector<float2> h(n);
+    for (int k2 = 0; k2 < r2; ++k2)
+        for (int n1 = 0; n1 < r1; ++n1) {
+            const long m = (long)n1 * k2 % n;
+            const double a = -2.0 * M_PI * (double)m / (double)n;
+            h[k2 * r1 + n1] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+    CK(s->twn.ensure(n));
+    CK(cudaMemcpyAsync(s->twn.p, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, s->st));
+    return 0;
+}
+
+int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz, const float *prop) {
+    if (n <= 1 || nz <= 0 || b <= 0) return fail(MSET_E_ARG, "invalid sizes n=%d nz=%d slice_binning=%d", n, nz, b);
+    Plan pl;
+    if (!plan_for(n, &pl))
+        return fail(MSET_E_UNSUPPORTED,
+                    "window size %d has no compiled kernel (supported: 24, 32, 48, 64, 96, 128, 160)", n);
+    if (b > nz) b = nz;  // STEP00_INIT.m:126-128
+    s->plan = pl;
+    s->n = n;
+    s->nz = nz;
+    s->b = b;
+    s->ns = (nz + b - 1) / b;
+    s->sigma = sigma;
+    s->dz = dz;
+    const size_t n2 = (size_t)n * n;
+    CK(s->pscr.ensure(n2));
+    CK(s->tmpc.ensure(n2 * 2));
+    int rc = upload_twiddles(s);
+    if (rc) return rc;
+    // propagator: host centred -> device -> scrambled / N^2
+    CK(cudaMemcpyAsync(s->tmpc.p, prop, sizeof(float2) * n2, cudaMemcpyHostToDevice, s->st));
+    CKL(launch_prep_prop(pl, reinterpret_cast<const float *>(s->tmpc.p), s->pscr.p, s->st), "prep_prop");
+    CK(s->err.ensure(64));
+    CK(s->counter.ensure(1));
+    return 0;
+}
+
+int ensure_save(mset_session *s, int slots) {
+    const size_t per = (size_t)(s->ns + 1) * s->n * s->n;
+    if (s->save_slots >= slots && s->save.n >= per * slots) return 0;
+    cudaError_t e = s->save.ensure(per * slots);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating saved-wave buffers");
+    s->save_slots = slots;
+    return 0;
+}
+
+int upload_tilt_probe(mset_session *s, TiltBufs &t, const float *probe) {
+    const size_t n2 = (size_t)s->n * s->n;
+    CK(t.Q.ensure(n2));
+    CK(cudaMemcpyAsync(s->tmpc.p, probe, sizeof(float2) * n2, cudaMemcpyHostToDevice, s->st));
+    CKL(launch_probe_to_q(s->plan, s->tmpc.p, t.Q.p, s->twn.p, s->st), "probe_to_q");
+    return 0;
+}
+
+int upload_tilt_measured(mset_session *s, TiltBufs &t, const float *meas) {
+    const size_t n2 = (size_t)s->n * s->n;
+    const size_t cnt = n2 * t.npos;
+    CK(t.amp.ensure(cnt));
+    if (cnt == 0) return 0;
+    CK(s->meas_tmp.ensure(std::max(s->meas_tmp.n, cnt)));
+    CK(cudaMemcpyAsync(s->meas_tmp.p, meas, sizeof(float) * cnt, cudaMemcpyHostToDevice, s->st));
+    CKL(launch_prep_amp(s->plan, s->meas_tmp.p, t.amp.p, t.npos, s->st), "prep_amp");
+    return 0;
+}
+
+int refresh_tilt_table(mset_session *s) {
+    const int J = (int)s->tilts.size();
+    s->h_tilts.assign(J, TiltDev{});
+    for (int j = 0; j < J; ++j) {
+        TiltBufs &t = s->tilts[j];
+        TiltDev &d = s->h_tilts[j];
+        d.V = t.V.p;
+        d.Q = t.Q.p;
+        d.amp = t.amp.p;
+        d.sx = t.sx.p;
+        d.sy = t.sy.p;
+        d.grad = t.grad.p;
+        d.qacc = t.qacc.p;
+        d.posdir = t.posdir.p;
+        d.err = s->err.p + j;
+        d.inten = s->inten.p ? s->inten.p + (size_t)s->pos_off[j] * s->n * s->n : nullptr;
+        d.npos = t.npos;
+    }
+    CK(s->d_tilts.ensure(J));
+    CK(cudaMemcpyAsync(s->d_tilts.p, s->h_tilts.data(), sizeof(TiltDev) * J, cudaMemcpyHostToDevice, s->st));
+    return 0;
+}
+
+int persistent_grid(mset_session *s, int items) {
+    // CTAs resident per SM for this kernel's shared memory and threads
+    const size_t per_sm_smem = 227 * 1024;
+    int by_smem = (int)(per_sm_smem / (s->plan.smem + 1024));
+    int by_thr = 2048 / s->plan.nt;
+    int c = std::max(1, std::min(by_smem, by_thr));
+    int g = s->sms * c;
+    return std::max(1, std::min(g, items));
+}
+
+LaunchArgs base_args(mset_session *s) {
+    LaunchArgs a{};
+    a.tilts = s->d_tilts.p;
+    a.items = s->items.p;
+    a.nitems = s->total_pos;
+    a.counter = s->counter.p;
+    a.save = s->save.p;
+    a.pscr = s->pscr.p;
+    a.twn = s->twn.p;
+    a.nz = s->nz;
+    a.b = s->b;
+    a.ns = s->ns;
+    a.sdz = s->sigma * s->dz;
+    a.center = (float)std::round((s->n + 1.0f) / 2.0f);  // mset.cu:83
+    a.step0 = s->step[0];
+    a.step1 = s->step[1];
+    a.step2 = s->step[2];
+    a.seq_tilt = 0;
+    return a;
+}
+
+int launch_queue(mset_session *s, int method, int adjoint, int mode) {
+    const int grid = persistent_grid(s, s->total_pos);
+    int rc = ensure_save(s, grid);
+    if (rc) return rc;
+    rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
+    LaunchArgs a = base_args(s);
+    CKL(launch_positions(s->plan, method, adjoint, mode, a, grid, s->st), "position kernel launch");
+    return 0;
+}
+
+int check_mode(int mode) {
+    if (mode != MSET_MODE_MSET && mode != MSET_MODE_SSET)
+        return fail(MSET_E_ARG, "The running mode is not correct (choose 'run_mset', 'run_sset', 'error_mset' or 'error_sset')");
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mset_last_error(void) { return g_err.c_str(); }
+const char *mset_version(void) { return "mset_b200 0.1 (sm_100a)"; }
+
+int mset_create(int device, mset_session **out) {
+    if (!out) return fail(MSET_E_ARG, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(MSET_E_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(MSET_E_ARG, "device %d out of range (%d devices)", device, ndev);
+    mset_session *s = new mset_session();
+    s->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(e, "session setup");
+    }
+    *out = s;
+    return 0;
+}
+
+int mset_destroy(mset_session *s) {
+    if (!s) return 0;
+    cudaSetDevice(s->device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    s->tilts.clear();
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return 0;
+}
+
+int mset_upload(mset_session *s, const mset_upload_args *a) {
+    if (!s || !a) return fail(MSET_E_ARG, "null argument");
+    if (!a->RVol || !a->init_wave2D || !a->prop2D || (!a->scan_xlist && a->num_scan_pos) ||
+        (!a->scan_ylist && a->num_scan_pos) || (!a->measured && a->num_scan_pos))
+        return fail(MSET_E_ARG, "null array in upload arguments");
+    if (a->num_scan_pos < 0) return fail(MSET_E_ARG, "num_scan_pos < 0");
+    if (a->N_scan_x <= 0 || a->N_scan_y <= 0) return fail(MSET_E_ARG, "N_scan_x and N_scan_y must be positive");
+    if (a->slice_binning <= 0) return fail(MSET_E_ARG, "slice_binning must be a positive integer");
+    int rc = set_device(s);
+    if (rc) return rc;
+    s->ready = false;
+    s->batch = false;
+    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
+    if (rc) return rc;
+    s->step[0] = a->step_size[0];
+    s->step[1] = a->step_size[1];
+    s->step[2] = a->step_size[2];
+    s->nsx = a->N_scan_x;
+    s->nsy = a->N_scan_y;
+    s->tilts.resize(1);
+    TiltBufs &t = s->tilts[0];
+    t.npos = a->num_scan_pos;
+    s->npos.assign(1, t.npos);
+    s->pos_off.assign(1, 0);
+    s->total_pos = t.npos;
+    const size_t n2 = (size_t)s->n * s->n;
+    CK(t.V.ensure(n2 * s->nz));
+    CK(cudaMemcpyAsync(t.V.p, a->RVol, sizeof(float) * n2 * s->nz, cudaMemcpyHostToDevice, s->st));
+    rc = upload_tilt_probe(s, t, a->init_wave2D);
+    if (rc) return rc;
+    CK(t.sx.ensure(std::max(1, t.npos)));
+    CK(t.sy.ensure(std::max(1, t.npos)));
+    if (t.npos) {
+        CK(cudaMemcpyAsync(t.sx.p, a->scan_xlist, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(t.sy.p, a->scan_ylist, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
+    }
+    rc = upload_tilt_measured(s, t, a->measured);
+    if (rc) return rc;
+    // work list for the forward-only pass
+    std::vector<int2> it(std::max(1, t.npos));
+    for (int p = 0; p < t.npos; ++p) it[p] = make_int2(0, p);
+    CK(s->items.ensure(it.size()));
+    CK(cudaMemcpyAsync(s->items.p, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * 64, s->st));  // mset.cu:38
+    CK(cudaStreamSynchronize(s->st));
+    s->ready = true;
+    return 0;
+}
+
+int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *probe_out, float *scan_x_out,
+                float *scan_y_out, float *error_out) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    int rc = check_mode(mode);
+    if (rc) return rc;
+    if (adjoint != MSET_ADJOINT_REF && adjoint != MSET_ADJOINT_EXACT) return fail(MSET_E_ARG, "bad adjoint mode");
+    if (!s->ready || s->batch) return fail(MSET_E_STATE, "run called before upload");
+    if (!rvol_out || !probe_out || !scan_x_out || !scan_y_out) return fail(MSET_E_ARG, "null output array");
+    rc = set_device(s);
+    if (rc) return rc;
+    rc = ensure_save(s, 1);
+    if (rc) return rc;
+    rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    LaunchArgs a = base_args(s);
+    CKL(launch_positions(s->plan, mode, adjoint, kSeq, a, 1, s->st), "sequential position kernel launch");
+    TiltBufs &t = s->tilts[0];
+    const size_t n2 = (size_t)s->n * s->n;
+    CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
+    CK(cudaMemcpyAsync(rvol_out, t.V.p, sizeof(float) * n2 * s->nz, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(probe_out, s->tmpc.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    if (t.npos) {
+        CK(cudaMemcpyAsync(scan_x_out, t.sx.p, sizeof(float) * t.npos, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaMemcpyAsync(scan_y_out, t.sy.p, sizeof(float) * t.npos, cudaMemcpyDeviceToHost, s->st));
+    }
+    double e = 0;
+    CK(cudaMemcpyAsync(&e, s->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (error_out) *error_out = (float)(e / ((double)s->nsx * s->nsy) / (double)n2);  // mex_main.cu:150
+    return 0;
+}
+
+int mset_run(mset_session *s, int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out,
+             float *error_out) {
+    return mset_run_ex(s, mode, MSET_ADJOINT_REF, rvol_out, probe_out, scan_x_out, scan_y_out, error_out);
+}
+
+int mset_error(mset_session *s, int mode, float *error_out) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    int rc = check_mode(mode);
+    if (rc) return rc;
+    if (!s->ready || s->batch) return fail(MSET_E_STATE, "error called before upload");
+    if (!error_out) return fail(MSET_E_ARG, "null output");
+    rc = set_device(s);
+    if (rc) return rc;
+    if (s->total_pos > 0) {
+        rc = launch_queue(s, mode, kREF, kErr);
+        if (rc) return rc;
+    }
+    double e = 0;
+    CK(cudaMemcpyAsync(&e, s->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    const double n2 = (double)s->n * s->n;
+    *error_out = (float)(e / ((double)s->nsx * s->nsy) / n2);  // mex_main.cu:179
+    return 0;
+}
+
+// ---- global-session shims --------------------------------------------------
+static mset_session *g_mex = nullptr;
+
+int mset_mex_upload(const mset_upload_args *a) {
+    if (!g_mex) {
+        int rc = mset_create(0, &g_mex);
+        if (rc) return rc;
+    }
+    return mset_upload(g_mex, a);
+}
+int mset_mex_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out, float *error_out) {
+    if (!g_mex) return fail(MSET_E_STATE, "run called before upload");
+    return mset_run(g_mex, mode, rvol_out, probe_out, scan_x_out, scan_y_out, error_out);
+}
+int mset_mex_error(int mode, float *error_out) {
+    if (!g_mex) return fail(MSET_E_STATE, "error called before upload");
+    return mset_error(g_mex, mode, error_out);
+}
+int mset_mex_clear(void) {
+    int rc = mset_destroy(g_mex);
+    g_mex = nullptr;
+    return rc;
+}
+
+// ---- batched method ---------------------------------------------------------
+int mset_batch_setup(mset_session *s, const mset_batch_args *a) {
+    if (!s || !a || !a->prop2D || !a->npos) return fail(MSET_E_ARG, "null argument");
+    if (a->ntilts <= 0) return fail(MSET_E_ARG, "ntilts must be positive");
+    if (a->method != MSET_MODE_MSET && a->method != MSET_MODE_SSET) return fail(MSET_E_ARG, "bad method");
+    if (a->adjoint != MSET_ADJOINT_REF && a->adjoint != MSET_ADJOINT_EXACT) return fail(MSET_E_ARG, "bad adjoint");
+    int rc = set_device(s);
+    if (rc) return rc;
+    s->ready = false;
+    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
+    if (rc) return rc;
+    s->method = a->method;
+    s->adjoint = a->adjoint;
+    for (int i = 0; i < 3; ++i) s->step[i] = a->step_size[i];
+    s->nsx = s->nsy = 1;
+    const int J = a->ntilts;
+    s->tilts.resize(J);
+    s->npos.assign(a->npos, a->npos + J);
+    s->pos_off.assign(J, 0);
+    s->total_pos = 0;
+    const size_t n2 = (size_t)s->n * s->n;
+    const int nsg = a->method == MSET_MODE_SSET ? 1 : s->ns;
+    std::vector<int2> it;
+    for (int j = 0; j < J; ++j) {
+        if (a->npos[j] < 0) return fail(MSET_E_ARG, "negative position count for tilt %d", j);
+        s->pos_off[j] = s->total_pos;
+        s->total_pos += a->npos[j];
+        TiltBufs &t = s->tilts[j];
+        t.npos = a->npos[j];
+        CK(t.V.ensure(n2 * s->nz));
+        CK(t.Q.ensure(n2));
+        CK(t.amp.ensure(n2 * t.npos));
+        CK(t.sx.ensure(std::max(1, t.npos)));
+        CK(t.sy.ensure(std::max(1, t.npos)));
+        CK(t.grad.ensure(n2 * nsg));
+        CK(t.qacc.ensure(n2 * 2));
+        CK(t.posdir.ensure(2 * std::max(1, t.npos)));
+        CK(cudaMemsetAsync(t.V.p, 0, sizeof(float) * n2 * s->nz, s->st));
+        for (int p = 0; p < t.npos; ++p) it.push_back(make_int2(j, p));
+    }
+    // position-major order inside each tilt; tilts follow each other so the
+    // active gradient accumulators stay in L2
+    if (it.empty()) it.push_back(make_int2(0, 0));
+    CK(s->items.ensure(it.size()));
+    CK(cudaMemcpyAsync(s->items.p, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice, s->st));
+    if ((size_t)J > 64) {
+        CK(s->err.ensure(J));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    s->batch = true;
+    s->ready = true;
+    return 0;
+}
+
+static int batch_ok(mset_session *s) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    if (!s->ready || !s->batch) return fail(MSET_E_STATE, "batched call before mset_batch_setup");
+    return set_device(s);
+}
+
+int mset_batch_set_tilt(mset_session *s, int j, const float *probe, const float *scan_x, const float *scan_y,
+                        const float *measured, const float *volume) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (j < 0 || j >= (int)s->tilts.size()) return fail(MSET_E_ARG, "tilt index %d out of range", j);
+    TiltBufs &t = s->tilts[j];
+    if (probe) {
+        rc = upload_tilt_probe(s, t, probe);
+        if (rc) return rc;
+    }
+    if (t.npos) {
+        if (scan_x) CK(cudaMemcpyAsync(t.sx.p, scan_x, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
+        if (scan_y) CK(cudaMemcpyAsync(t.sy.p, scan_y, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
+        if (measured) {
+            rc = upload_tilt_measured(s, t, measured);
+            if (rc) return rc;
+        }
+    }
+    if (volume) {
+        CK(cudaMemcpyAsync(t.V.p, volume, sizeof(float) * (size_t)s->n * s->n * s->nz, cudaMemcpyHostToDevice,
+                           s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_set_volume(mset_session *s, int j, const float *volume) {
+    if (!volume) return fail(MSET_E_ARG, "null volume");
+    return mset_batch_set_tilt(s, j, nullptr, nullptr, nullptr, nullptr, volume);
+}
+
+static int batch_zero(mset_session *s) {
+    const size_t n2 = (size_t)s->n * s->n;
+    const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
+    for (auto &t : s->tilts) {
+        CK(cudaMemsetAsync(t.grad.p, 0, sizeof(double) * n2 * nsg, s->st));
+        CK(cudaMemsetAsync(t.qacc.p, 0, sizeof(double) * n2 * 2, s->st));
+    }
+    CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * s->tilts.size(), s->st));
+    return 0;
+}
+
+static int batch_pass(mset_session *s) {
+    int rc = batch_zero(s);
+    if (rc) return rc;
+    if (s->total_pos == 0) return 0;
+    return launch_queue(s, s->method, s->adjoint, kBatch);
+}
+
+int mset_batch_gradient(mset_session *s, double *grad_out, double *probe_out, double *posdir_out, double *err_out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    rc = batch_pass(s);
+    if (rc) return rc;
+    const size_t n2 = (size_t)s->n * s->n;
+    const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
+    const int J = (int)s->tilts.size();
+    for (int j = 0; j < J; ++j) {
+        TiltBufs &t = s->tilts[j];
+        if (grad_out)
+            CK(cudaMemcpyAsync(grad_out + (size_t)j * nsg * n2, t.grad.p, sizeof(double) * nsg * n2,
+                               cudaMemcpyDeviceToHost, s->st));
+        if (probe_out) {
+            // device layout is scrambled; the caller gets standard FFT order
+            std::vector<double> tmp(2 * n2);
+            CK(cudaMemcpyAsync(tmp.data(), t.qacc.p, sizeof(double) * 2 * n2, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            const int n = s->n, r1 = s->plan.r1, r2 = n / r1;
+            double *o = probe_out + (size_t)j * 2 * n2;
+            for (int ly = 0; ly < n; ++ly)
+                for (int lx = 0; lx < n; ++lx) {
+                    const int ky = ly / r1 + r2 * (ly % r1), kx = lx / r1 + r2 * (lx % r1);
+                    o[2 * ((size_t)ky * n + kx)] = tmp[2 * ((size_t)ly * n + lx)];
+                    o[2 * ((size_t)ky * n + kx) + 1] = tmp[2 * ((size_t)ly * n + lx) + 1];
+                }
+        }
+        if (posdir_out && t.npos)
+            CK(cudaMemcpyAsync(posdir_out + 2 * (size_t)s->pos_off[j], t.posdir.p, sizeof(double) * 2 * t.npos,
+                               cudaMemcpyDeviceToHost, s->st));
+    }
+    if (err_out) CK(cudaMemcpyAsync(err_out, s->err.p, sizeof(double) * J, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_error(mset_session *s, double *err_out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * s->tilts.size(), s->st));
+    if (s->total_pos) {
+        rc = launch_queue(s, s->method, kREF, kErr);
+        if (rc) return rc;
+    }
+    if (err_out) CK(cudaMemcpyAsync(err_out, s->err.p, sizeof(double) * s->tilts.size(), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_simulate(mset_session *s, float *inten_out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!inten_out) return fail(MSET_E_ARG, "null output");
+    const size_t n2 = (size_t)s->n * s->n;
+    CK(s->inten.ensure(std::max<size_t>(1, n2 * s->total_pos)));
+    if (s->total_pos) {
+        rc = launch_queue(s, s->method, kREF, kSim);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(inten_out, s->inten.p, sizeof(float) * n2 * s->total_pos, cudaMemcpyDeviceToHost, s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    s->inten.release();
+    return refresh_tilt_table(s);
+}
+
+int mset_batch_apply(mset_session *s) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    CKL(launch_apply_batch(s->n, s->nz, s->b, s->ns, s->method, s->step[0], s->step[1], s->step[2],
+                           s->h_tilts.data(), (int)s->tilts.size(), s->st),
+        "apply");
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_get_tilt(mset_session *s, int j, float *volume, float *probe, float *scan_x, float *scan_y) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (j < 0 || j >= (int)s->tilts.size()) return fail(MSET_E_ARG, "tilt index %d out of range", j);
+    TiltBufs &t = s->tilts[j];
+    const size_t n2 = (size_t)s->n * s->n;
+    if (volume) CK(cudaMemcpyAsync(volume, t.V.p, sizeof(float) * n2 * s->nz, cudaMemcpyDeviceToHost, s->st));
+    if (probe) {
+        CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
+        CK(cudaMemcpyAsync(probe, s->tmpc.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (scan_x && t.npos) CK(cudaMemcpyAsync(scan_x, t.sx.p, sizeof(float) * t.npos, cudaMemcpyDeviceToHost, s->st));
+    if (scan_y && t.npos) CK(cudaMemcpyAsync(scan_y, t.sy.p, sizeof(float) * t.npos, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (reps <= 0 || !ms_per_pass) return fail(MSET_E_ARG, "bad arguments");
+    CK(cudaEventRecord(s->ev0, s->st));
+    for (int r = 0; r < reps; ++r) {
+        rc = batch_pass(s);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(s->ev1, s->st));
+    CK(cudaEventSynchronize(s->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *ms_per_pass = ms / reps;
+    return 0;
+}
+
+int mset_batch_launch_count(mset_session *s) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    return 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// mset_dispatch.cu -- window-size dispatch and the size-independent
+// kernels of the batched update.
+#include <algorithm>
+#include "mset_kernels.cuh"
+
+namespace mset {
+
+#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(96) X(128) X(160)
+#define X(N_) extern const GeoOps kGeo##N_;
+MSET_GEOS(X)
+#undef X
+
+static const GeoOps *find_geo(int n) {
+#define X(N_) \
+    if (n == N_) return &kGeo##N_;
+    MSET_GEOS(X)
+#undef X
+    return nullptr;
+}
+
+bool plan_for(int n, Plan *p) {
+    const GeoOps *g = find_geo(n);
+    if (!g) return false;
+    p->n = g->n;
+    p->r1 = g->r1;
+    p->nt = g->nt;
+    p->smem = g->smem;
+    p->ctas_per_sm = 0;
+    p->ops = g;
+    return true;
+}
+
+int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,
+                     cudaStream_t st) {
+    return pl.ops->positions(method, adjoint, mode, a, grid, st);
+}
+int launch_prep_amp(const Plan &pl, const float *meas, float *amp, long npos, cudaStream_t st) {
+    return pl.ops->prep_amp(meas, amp, npos, st);
+}
+int launch_prep_prop(const Plan &pl, const float *prop, float2 *pscr, cudaStream_t st) {
+    return pl.ops->prep_prop(prop, pscr, st);
+}
+int launch_probe_to_q(const Plan &pl, const float2 *probe, float2 *q, const float2 *twn, cudaStream_t st) {
+    return pl.ops->probe_q(true, probe, q, twn, st);
+}
+int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const float2 *twn, cudaStream_t st) {
+    return pl.ops->probe_q(false, q, probe, twn, st);
+}
+
+// batched update: V += step0 * G (slab-replicated), Q -= step1 * qacc,
+// positions += step2 * posdir
+__global__ void k_apply_volume(float *V, const double *g, int n2, int nz, int b, float step0) {
+    const long total = (long)nz * n2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(i / n2);
+        const int l = (int)(i % n2);
+        const int s = z / b;
+        V[i] += step0 * (float)g[(long)s * n2 + l];
+    }
+}
+__global__ void k_apply_probe(float2 *Q, const double *qacc, int n2, float step1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+        float2 q = Q[i];
+        q.x -= step1 * (float)qacc[2 * i];
+        q.y -= step1 * (float)qacc[2 * i + 1];
+        Q[i] = q;
+    }
+}
+__global__ void k_apply_pos(float *sx, float *sy, const double *pd, int npos, float step2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npos; i += gridDim.x * blockDim.x) {
+        sx[i] += step2 * (float)pd[2 * i];
+        sy[i] += step2 * (float)pd[2 * i + 1];
+    }
+}
+
+int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,
+                       const TiltDev *tilts, int ntilts, cudaStream_t st) {
+    (void)ns;
+    const int n2 = n * n;
+    const int bb = method == kSSET ? nz : b;
+    for (int j = 0; j < ntilts; ++j) {
+        const TiltDev &t = tilts[j];
+        k_apply_volume<<<592, 256, 0, st>>>(t.V, t.grad, n2, nz, bb, step0);
+        k_apply_probe<<<64, 256, 0, st>>>(t.Q, t.qacc, n2, step1);
+        k_apply_pos<<<8, 256, 0, st>>>(t.sx, t.sy, t.posdir, t.npos, step2);
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace mset

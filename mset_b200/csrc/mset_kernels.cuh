@@ -1,0 +1,76 @@
+// mset_kernels.cuh -- internal interface between the C-ABI host layer
+// (mset_api.cu) and the fused multislice kernels (mset_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mset {
+
+enum Method { kMSET = 1, kSSET = 2 };
+enum Adjoint { kREF = 0, kEXACT = 1 };
+// what one launch does with each position
+enum Mode {
+    kSeq = 0,    // reference semantics: update volume, probe and position after every position
+    kBatch = 1,  // fixed state, accumulate FP64 gradients over positions
+    kErr = 2,    // forward + error only (run_error_mset / run_error_sset)
+    kSim = 3     // forward + write |Psi|^2 (centred layout)
+};
+
+// one tilt: all buffers on the device
+struct TiltDev {
+    float *V;            // [nz][n][n] beam-frame potential (kSeq: updated in place)
+    float2 *Q;           // [n][n] scrambled F^{-1}(probe)  (kSeq: updated in place)
+    const float *amp;    // [npos][n][n] scrambled sqrt(ifftshift(I_meas))
+    float *sx, *sy;      // [npos] 1-based scan coordinates (kSeq: updated in place)
+    double *grad;        // kBatch: [ns][n][n] sum_p Re(g)   (natural layout)
+    double *qacc;        // kBatch: [n][n][2] scrambled sum_p F^{-1}(chi0) fs(-s)
+    double *posdir;      // kBatch: [npos][2]
+    double *err;         // [1] sum over positions and pixels of (A-M)^2
+    float *inten;        // kSim: [npos][n][n] centred |Psi|^2
+    int npos;
+    int pad_;
+};
+
+struct LaunchArgs {
+    const TiltDev *tilts;   // device array
+    const int2 *items;      // device array of (tilt, position), kBatch/kErr/kSim
+    int nitems;
+    unsigned *counter;      // work-queue counter (zeroed before the launch)
+    float2 *save;           // per-CTA saved waves: [grid][ns+1][n][n]
+    const float2 *pscr;     // propagator / N^2, scrambled layout
+    const float2 *twn;      // [n] twiddles e^{-2 pi i m/N} as [k2][n1]
+    int nz, b, ns;
+    float sdz;              // sigma * dz
+    float center;           // round((N+1)/2)
+    float step0, step1, step2;
+    int seq_tilt;           // kSeq: index of the tilt to run
+};
+
+// per-window-size kernel table (one translation unit per size, geo_<N>.cu)
+struct GeoOps {
+    int n, r1, nt;
+    size_t smem;
+    int (*positions)(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st);
+    int (*prep_amp)(const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
+    int (*prep_prop)(const float *prop_centred, float2 *pscr, cudaStream_t st);
+    int (*probe_q)(bool to_q, const float2 *in, float2 *out, const float2 *twn, cudaStream_t st);
+};
+
+// host-side launchers (return cudaError_t as int)
+struct Plan {
+    int n, r1, nt;
+    size_t smem;
+    int ctas_per_sm;
+    const GeoOps *ops;
+};
+bool plan_for(int n, Plan *p);
+int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,
+                     cudaStream_t st);
+int launch_prep_amp(const Plan &pl, const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
+int launch_prep_prop(const Plan &pl, const float *prop_centred, float2 *pscr, cudaStream_t st);
+int launch_probe_to_q(const Plan &pl, const float2 *probe, float2 *q, const float2 *twn, cudaStream_t st);
+int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const float2 *twn, cudaStream_t st);
+int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,
+                       const TiltDev *tilts_host, int ntilts, cudaStream_t st);
+
+}  // namespace mset

@@ -1,0 +1,534 @@
+// mset_kernels_impl.cuh -- fused per-position multislice forward / adjoint kernels
+// for sm_100a.
+//
+// One CTA owns one probe position at a time; the wave stays in shared memory
+// for the whole forward pass, far field and adjoint.  Per slab it costs six
+// shared-memory passes forward and six backward (see fft_core.cuh), with the
+// transmission exp(i sigma dz sum V), the propagator product, the saved-wave
+// store, the gradient product and the far-field residual fused into the
+// passes that border them.
+//
+// Reference semantics (kSeq) follow src/CUDA/mset.cu:80-334 (MSET) and
+// :345-546 (SSET): volume, probe and scan position are updated after every
+// position, inside the same launch.  kBatch keeps the state fixed and
+// accumulates the gradients of every position of every tilt in FP64
+// (the batched method).  kErr is run_error_mset/_sset (mset.cu:557-810).
+#pragma once
+#include "fft_core.cuh"
+#include "mset_kernels.cuh"
+
+namespace mset {
+
+// pi as hard-coded in the reference's Fourier shift factor (utility.cu:790)
+#define MSET_REF_PI 3.1415926f
+
+template <int NT>
+__device__ __forceinline__ void block_sum2(double &a, double &b, double *red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        red[2 * w] = a;
+        red[2 * w + 1] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sa = 0, sb = 0;
+        for (int i = 0; i < (NT + 31) / 32; ++i) {
+            sa += red[2 * i];
+            sb += red[2 * i + 1];
+        }
+        red[0] = sa;
+        red[1] = sb;
+    }
+    __syncthreads();
+    a = red[0];
+    b = red[1];
+    __syncthreads();
+}
+
+// frequency index n(k) of the reference shift factor grid: location k of the
+// ifftshifted grid carries n = ((k - ceil(N/2)) mod N) - N/2
+// (utility.cu:786-787 followed by circular_shift2D_dev by ceil(N/2)).
+__device__ __forceinline__ float shift_grid(int k, int n) {
+    const int h = (n + 1) / 2;
+    int i = k - h;
+    if (i < 0) i += n;
+    return (float)i - (float)n * 0.5f;
+}
+
+template <class G, int METHOD, int ADJ, int MODE>
+struct PositionKernel {
+    static constexpr int N = G::N, NN = G::N * G::N;
+
+    // transmission of slab s at (y, x): exp(i sdz sum_{z in slab} V)
+    // (mset.cu:134-153 / STEP02_FORWARD_4D.m:12-20; SSET: all z, mset.cu:391-404)
+    static __device__ __forceinline__ float2 trans(const LaunchArgs &a, const float *V, int s, int y, int x) {
+        int z0, z1;
+        if constexpr (METHOD == kSSET) {
+            z0 = 0;
+            z1 = a.nz;
+        } else {
+            z0 = s * a.b;
+            z1 = min(z0 + a.b, a.nz);
+        }
+        const float *p = V + (size_t)y * N + x;
+        float acc = 0.f;
+        for (int z = z0; z < z1; ++z) acc += p[(size_t)z * NN];
+        float sn, cs;
+        sincosf(a.sdz * acc, &sn, &cs);
+        return make_float2(cs, sn);
+    }
+
+    static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, const float2 *tw,
+                               float2 *e1, float2 *e2, double *red, float2 *save) {
+        const int ns = METHOD == kSSET ? 1 : a.ns;
+        float *V = t.V;
+        const float sxp = t.sx[p], syp = t.sy[p];
+        const float s1 = syp - a.center, s2 = sxp - a.center;  // mset.cu:121
+        // separable Fourier shift factor, indexed by scrambled location
+        for (int L = threadIdx.x; L < N; L += G::NT) {
+            const float nf = shift_grid(G::scr(L), N);
+            float sn, cs;
+            sincosf(2.0f * MSET_REF_PI * (s1 * nf / (float)N), &sn, &cs);
+            e1[L] = make_float2(cs, sn);
+            sincosf(2.0f * MSET_REF_PI * (s2 * nf / (float)N), &sn, &cs);
+            e2[L] = make_float2(cs, sn);
+        }
+        __syncthreads();
+
+        // ---- incident wave psi0 = F(Q . fs)  (mset.cu:110-131) ----
+        col_passB<G, 0, -1>(buf, [&](int y0, int x, float2 *v) {
+            const float2 *q = t.Q + (size_t)y0 * N + x;
+            const float2 ex = e2[x];
+#pragma unroll
+            for (int j = 0; j < G::R1; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
+        });
+        __syncthreads();
+        col_passA<G, -1, false>(buf, tw);
+        __syncthreads();
+        row_passB<G, -1>(buf);
+        __syncthreads();
+        if constexpr (MODE == kSim || MODE == kErr) {
+            row_passA<G, -1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
+#pragma unroll
+                for (int j = 0; j < G::R2; ++j) v[j] = cmul(v[j], trans(a, V, 0, y, n1 + G::R1 * j));
+            });
+        } else {
+            row_passA<G, -1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
+                float2 *sv = save + (size_t)y * N + n1;
+#pragma unroll
+                for (int j = 0; j < G::R2; ++j) {
+                    sv[G::R1 * j] = v[j];
+                    v[j] = cmul(v[j], trans(a, V, 0, y, n1 + G::R1 * j));
+                }
+            });
+        }
+        __syncthreads();
+
+        // ---- forward slabs (mset.cu:157-183) ----
+        if constexpr (METHOD == kMSET) {
+            for (int s = 0; s < ns; ++s) {
+                row_passB<G, -1>(buf);
+                __syncthreads();
+                col_passA<G, -1, true>(buf, tw);
+                __syncthreads();
+                col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
+                    const float2 *pp = a.pscr + (size_t)y0 * N + x;
+#pragma unroll
+                    for (int j = 0; j < G::R1; ++j) v[j] = cmul(v[j], __ldg(pp + (size_t)j * N));
+                });
+                __syncthreads();
+                col_passA<G, +1, false>(buf, tw);
+                __syncthreads();
+                row_passB<G, +1>(buf);
+                __syncthreads();
+                const bool last = s + 1 == ns;
+                row_passA<G, +1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
+                    if constexpr (MODE != kSim && MODE != kErr) {
+                        float2 *sv = save + (size_t)(s + 1) * NN + (size_t)y * N + n1;
+#pragma unroll
+                        for (int j = 0; j < G::R2; ++j) sv[G::R1 * j] = v[j];
+                    }
+                    if (!last) {
+#pragma unroll
+                        for (int j = 0; j < G::R2; ++j) v[j] = cmul(v[j], trans(a, V, s + 1, y, n1 + G::R1 * j));
+                    }
+                });
+                __syncthreads();
+            }
+        }
+
+        // ---- far field, error, residual (mset.cu:186-227) ----
+        row_passB<G, -1>(buf);
+        __syncthreads();
+        col_passA<G, -1, true>(buf, tw);
+        __syncthreads();
+        double err = 0.0;
+        const float *amp = t.amp + (size_t)p * NN;
+        if constexpr (MODE == kSim || MODE == kErr) {
+            col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+                for (int j = 0; j < G::R1; ++j) {
+                    const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
+                    if constexpr (MODE == kSim) {
+                        // centred (MATLAB) layout: row r with (r + ceil(N/2)) mod N = ky
+                        const int h = (N + 1) / 2;
+                        int r = G::scr(y0 + j) - h, c = G::scr(x) - h;
+                        if (r < 0) r += N;
+                        if (c < 0) c += N;
+                        t.inten[(size_t)p * NN + (size_t)r * N + c] = a2;
+                    } else {
+                        const float A = sqrtf(a2 + 1e-30f);
+                        const float M = __ldg(amp + (size_t)(y0 + j) * N + x);
+                        const float d = A - M;
+                        err += (double)(d * d);
+                    }
+                }
+            });
+            if constexpr (MODE == kErr) {
+                double dummy = 0.0;
+                block_sum2<G::NT>(err, dummy, red);
+                if (threadIdx.x == 0) atomicAdd(t.err, err);
+            }
+            __syncthreads();
+            return;
+        } else {
+            col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
+                const float2 *pp = a.pscr + (size_t)y0 * N + x;
+#pragma unroll
+                for (int j = 0; j < G::R1; ++j) {
+                    const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
+                    const float A = sqrtf(a2 + 1e-30f);
+                    const float M = __ldg(amp + (size_t)(y0 + j) * N + x);
+                    const float d = A - M;
+                    err += (double)(d * d);
+                    float2 r = cscale(v[j], 1.0f - M / A);
+                    if constexpr (METHOD == kMSET) {
+                        r = cmulc(r, __ldg(pp + (size_t)j * N));  // r * conj(P) / N^2
+                    } else {
+                        r = cscale(r, 1.0f / (float)NN);
+                    }
+                    v[j] = r;
+                }
+            });
+            __syncthreads();
+        }
+
+        // ---- adjoint (mset.cu:232-271; STEP03_BACK.m:12-26) ----
+        for (int s = ns - 1; s >= 0; --s) {
+            col_passA<G, +1, false>(buf, tw);
+            __syncthreads();
+            row_passB<G, +1>(buf);
+            __syncthreads();
+            auto gradop = [&](int y, int n1, float2 *v) {
+                // REF: the wave saved after slab s (mset.cu:248-251); EXACT: the wave entering slab s
+                const int ws = (METHOD == kSSET || ADJ == kEXACT) ? s : s + 1;
+                const float2 *sv = save + (size_t)ws * NN + (size_t)y * N + n1;
+#pragma unroll
+                for (int j = 0; j < G::R2; ++j) {
+                    const int x = n1 + G::R1 * j;
+                    const float2 T = trans(a, V, s, y, x);
+                    const float2 psi = sv[G::R1 * j];
+                    // g = i conj(T) conj(psi) chi
+                    const float2 u = cmulc(cmulc(v[j], T), psi);
+                    const float gre = -u.y;  // Re(i u)
+                    if constexpr (MODE == kSeq) {
+                        int z0, z1;
+                        if constexpr (METHOD == kSSET) {
+                            z0 = 0;
+                            z1 = a.nz;
+                        } else {
+                            z0 = s * a.b;
+                            z1 = min(z0 + a.b, a.nz);
+                        }
+                        // RVol += step0 * Re(grad), slab-replicated (mset.cu:273-284)
+                        const float du = a.step0 * gre;
+                        for (int z = z0; z < z1; ++z) V[(size_t)z * NN + (size_t)y * N + x] += du;
+                    } else {
+                        atomicAdd(t.grad + (size_t)s * NN + (size_t)y * N + x, (double)gre);
+                    }
+                    v[j] = cmulc(v[j], T);  // chi <- conj(T) chi
+                }
+            };
+            if (s > 0) {
+                row_passA<G, +1, -1>(buf, tw, gradop);
+                __syncthreads();
+                row_passB<G, -1>(buf);
+                __syncthreads();
+                col_passA<G, -1, true>(buf, tw);
+                __syncthreads();
+                col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
+                    const float2 *pp = a.pscr + (size_t)y0 * N + x;
+#pragma unroll
+                    for (int j = 0; j < G::R1; ++j) v[j] = cmulc(v[j], __ldg(pp + (size_t)j * N));
+                });
+                __syncthreads();
+            } else {
+                row_passA<G, +1, 0>(buf, tw, gradop);
+                __syncthreads();
+            }
+        }
+        // buf now holds chi0 (real space, natural order); save[0] holds psi0.
+
+        // ---- scan-position direction, REF: finite differences of conj(psi0)
+        //      (mset.cu:316-327; utility.cu:829-876) ----
+        double pdx = 0.0, pdy = 0.0;
+        if constexpr (ADJ == kREF) {
+            for (int i = threadIdx.x; i < NN; i += G::NT) {
+                const int y = i / N, x = i % N;
+                const float2 c0 = buf[G::at(y, x)];
+                const float2 *f = save + (size_t)y * N + x;
+                float2 dx, dy;
+                if (x == 0) dx = csub(f[1], f[0]);
+                else if (x == N - 1) dx = csub(f[0], f[-1]);
+                else dx = cscale(csub(f[1], f[-1]), 0.5f);
+                if (y == 0) dy = csub(f[N], f[0]);
+                else if (y == N - 1) dy = csub(f[0], f[-N]);
+                else dy = cscale(csub(f[N], f[-N]), 0.5f);
+                // Re(conj(d) * chi0)
+                pdx += (double)(dx.x * c0.x + dx.y * c0.y);
+                pdy += (double)(dy.x * c0.x + dy.y * c0.y);
+            }
+        }
+        __syncthreads();
+
+        // ---- probe direction: d = F^{-1}(chi0) fs(-s), accumulated in the
+        //      F^{-1}(probe) domain (mset.cu:288-312) ----
+        row_passA<G, 0, +1>(buf, tw, NoOp{});
+        __syncthreads();
+        row_passB<G, +1>(buf);
+        __syncthreads();
+        col_passA<G, +1, true>(buf, tw);
+        __syncthreads();
+        const float inv = 1.0f / (float)NN;
+        col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
+            const float2 ex = e2[x];
+            const float kx = 2.0f * MSET_REF_PI * shift_grid(G::scr(x), N) / (float)N;
+#pragma unroll
+            for (int j = 0; j < G::R1; ++j) {
+                const size_t li = (size_t)(y0 + j) * N + x;
+                const float2 fs = cmul(e1[y0 + j], ex);
+                const float2 d = cscale(cmulc(v[j], fs), inv);
+                if constexpr (ADJ == kEXACT) {
+                    // spectral derivative of psi0 w.r.t. the scan coordinates
+                    const float2 qf = cmul(t.Q[li], fs);
+                    const float ky = 2.0f * MSET_REF_PI * shift_grid(G::scr(y0 + j), N) / (float)N;
+                    // X = Q fs (i kappa); -Re(conj(X) Y)
+                    const float2 Xx = make_float2(-qf.y * kx, qf.x * kx);
+                    const float2 Xy = make_float2(-qf.y * ky, qf.x * ky);
+                    pdx -= (double)(Xx.x * v[j].x + Xx.y * v[j].y);
+                    pdy -= (double)(Xy.x * v[j].x + Xy.y * v[j].y);
+                }
+                if constexpr (MODE == kSeq) {
+                    float2 q = t.Q[li];
+                    q.x -= a.step1 * d.x;
+                    q.y -= a.step1 * d.y;
+                    t.Q[li] = q;
+                } else {
+                    atomicAdd(t.qacc + 2 * li, (double)d.x);
+                    atomicAdd(t.qacc + 2 * li + 1, (double)d.y);
+                }
+            }
+        });
+        block_sum2<G::NT>(pdx, pdy, red);
+        double dummy = 0.0;
+        block_sum2<G::NT>(err, dummy, red);
+        if (threadIdx.x == 0) {
+            atomicAdd(t.err, err);
+            if constexpr (MODE == kSeq) {
+                t.sx[p] = sxp + a.step2 * (float)pdx;  // mset.cu:322
+                t.sy[p] = syp + a.step2 * (float)pdy;  // mset.cu:327
+            } else {
+                t.posdir[2 * p] = pdx;
+                t.posdir[2 * p + 1] = pdy;
+            }
+        }
+        __syncthreads();
+    }
+};
+
+template <class G>
+__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *twn) {
+    for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
+}
+
+template <class G, int METHOD, int ADJ, int MODE>
+__global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a) {
+    extern __shared__ __align__(16) float2 smem[];
+    float2 *buf = smem;
+    float2 *tw = buf + G::N * G::S;
+    float2 *e1 = tw + G::N;
+    float2 *e2 = e1 + G::N;
+    double *red = reinterpret_cast<double *>(e2 + G::N);
+    __shared__ int s_item;
+    load_twiddles<G>(tw, a.twn);
+    const int nsave = (METHOD == kSSET ? 1 : a.ns) + 1;
+    float2 *save = a.save + (size_t)blockIdx.x * nsave * G::N * G::N;
+    __syncthreads();
+    using K = PositionKernel<G, METHOD, ADJ, MODE>;
+    if constexpr (MODE == kSeq) {
+        const TiltDev &t = a.tilts[a.seq_tilt];
+        for (int p = 0; p < t.npos; ++p) K::run(a, t, p, buf, tw, e1, e2, red, save);
+    } else {
+        for (;;) {
+            if (threadIdx.x == 0) s_item = (int)atomicAdd(a.counter, 1u);
+            __syncthreads();
+            const int it = s_item;
+            __syncthreads();
+            if (it >= a.nitems) break;
+            const int2 tp = a.items[it];
+            K::run(a, a.tilts[tp.x], tp.y, buf, tw, e1, e2, red, save);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// preparation kernels
+// ---------------------------------------------------------------------------
+template <class G>
+__global__ void k_prep_amp(const float *meas, float *amp, long npos) {
+    // amp[p][Ly][Lx] = sqrt(ifftshift(I)[scr(Ly)][scr(Lx)])  (mset.cu:206-210)
+    const long total = npos * (long)G::N * G::N;
+    const int h = (G::N + 1) / 2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long p = i / ((long)G::N * G::N);
+        const int l = (int)(i % ((long)G::N * G::N));
+        const int Ly = l / G::N, Lx = l % G::N;
+        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        if (r < 0) r += G::N;
+        if (c < 0) c += G::N;
+        amp[i] = sqrtf(meas[p * G::N * G::N + (long)r * G::N + c]);
+    }
+}
+
+template <class G>
+__global__ void k_prep_prop(const float2 *prop, float2 *pscr) {
+    // pscr[Ly][Lx] = ifftshift(prop)[scr(Ly)][scr(Lx)] / N^2  (mex_main.cu:80-83)
+    const int h = (G::N + 1) / 2;
+    const float inv = 1.0f / (float)(G::N * G::N);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G::N * G::N; i += gridDim.x * blockDim.x) {
+        const int Ly = i / G::N, Lx = i % G::N;
+        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        if (r < 0) r += G::N;
+        if (c < 0) c += G::N;
+        pscr[i] = cscale(prop[r * G::N + c], inv);
+    }
+}
+
+// Q = F^{-1}(probe) (scrambled) and probe = F(Q) (natural); one CTA.
+template <class G, bool TO_Q>
+__global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out, const float2 *twn) {
+    extern __shared__ __align__(16) float2 smem[];
+    float2 *buf = smem;
+    float2 *tw = buf + G::N * G::S;
+    load_twiddles<G>(tw, twn);
+    __syncthreads();
+    constexpr int N = G::N;
+    if constexpr (TO_Q) {
+        for (int i = threadIdx.x; i < N * N; i += G::NT) buf[G::at(i / N, i % N)] = in[i];
+        __syncthreads();
+        row_passA<G, 0, +1>(buf, tw, NoOp{});
+        __syncthreads();
+        row_passB<G, +1>(buf);
+        __syncthreads();
+        col_passA<G, +1, true>(buf, tw);
+        __syncthreads();
+        const float inv = 1.0f / (float)(N * N);
+        col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+            for (int j = 0; j < G::R1; ++j) out[(size_t)(y0 + j) * N + x] = cscale(v[j], inv);
+        });
+    } else {
+        col_passB<G, 0, -1>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+            for (int j = 0; j < G::R1; ++j) v[j] = in[(size_t)(y0 + j) * N + x];
+        });
+        __syncthreads();
+        col_passA<G, -1, false>(buf, tw);
+        __syncthreads();
+        row_passB<G, -1>(buf);
+        __syncthreads();
+        row_passA<G, -1, 0>(buf, tw, [&](int y, int n1, float2 *v) {
+#pragma unroll
+            for (int j = 0; j < G::R2; ++j) out[(size_t)y * N + n1 + G::R1 * j] = v[j];
+        });
+    }
+}
+
+
+template <class G>
+inline size_t smem_bytes() {
+    return sizeof(float2) * ((size_t)G::N * G::S + 3 * G::N) + sizeof(double) * 2 * ((G::NT + 31) / 32);
+}
+
+template <class G, int METHOD, int ADJ, int MODE>
+inline int launch_one(const LaunchArgs &a, int grid, cudaStream_t st) {
+    auto k = k_positions<G, METHOD, ADJ, MODE>;
+    const size_t sm = smem_bytes<G>();
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return (int)e;
+    k<<<grid, G::NT, sm, st>>>(a);
+    return (int)cudaGetLastError();
+}
+
+template <class G>
+int geo_positions(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st) {
+    if (mode == kErr || mode == kSim) adjoint = kREF;
+#define MSET_L(M, A, MO) \
+    if (method == M && adjoint == A && mode == MO) return launch_one<G, M, A, MO>(a, grid, st);
+    MSET_L(kMSET, kREF, kSeq) MSET_L(kMSET, kREF, kBatch) MSET_L(kMSET, kEXACT, kSeq) MSET_L(kMSET, kEXACT, kBatch)
+    MSET_L(kSSET, kREF, kSeq) MSET_L(kSSET, kREF, kBatch) MSET_L(kSSET, kEXACT, kSeq) MSET_L(kSSET, kEXACT, kBatch)
+    MSET_L(kMSET, kREF, kErr) MSET_L(kSSET, kREF, kErr) MSET_L(kMSET, kREF, kSim) MSET_L(kSSET, kREF, kSim)
+#undef MSET_L
+    return (int)cudaErrorInvalidValue;
+}
+
+template <class G>
+int geo_prep_amp(const float *meas, float *amp, long npos, cudaStream_t st) {
+    k_prep_amp<G><<<1184, 256, 0, st>>>(meas, amp, npos);
+    return (int)cudaGetLastError();
+}
+
+template <class G>
+int geo_prep_prop(const float *prop, float2 *pscr, cudaStream_t st) {
+    k_prep_prop<G><<<148, 256, 0, st>>>(reinterpret_cast<const float2 *>(prop), pscr);
+    return (int)cudaGetLastError();
+}
+
+template <class G>
+int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cudaStream_t st) {
+    const size_t sm = smem_bytes<G>();
+    if (to_q) {
+        auto k = k_probe_q<G, true>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return (int)e;
+        k<<<1, G::NT, sm, st>>>(in, out, twn);
+    } else {
+        auto k = k_probe_q<G, false>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return (int)e;
+        k<<<1, G::NT, sm, st>>>(in, out, twn);
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace mset
+
+// one translation unit per window size defines its table entry
+#define MSET_DEFINE_GEO(N_, R1_, NT_, MINB_)                                           \
+    namespace mset {                                                                   \
+    using Geo##N_ = Geo<N_, R1_, NT_, MINB_>;                                               \
+    extern const GeoOps kGeo##N_ = {N_,                                                \
+                                    R1_,                                               \
+                                    NT_,                                               \
+                                    smem_bytes<Geo##N_>(),                             \
+                                    &geo_positions<Geo##N_>,                           \
+                                    &geo_prep_amp<Geo##N_>,                            \
+                                    &geo_prep_prop<Geo##N_>,                           \
+                                    &geo_probe_q<Geo##N_>};                            \
+    }

@@ -1,0 +1,204 @@
+"""Host-side mirror of the reference's MEX interface (src/CUDA/mex_main.cu).
+
+Two layers:
+
+* :class:`Session` -- an explicit handle over the C ABI with C-order numpy
+  arrays (volume ``[nz][n][n]`` float32, probe ``[n][n]`` complex64, measured
+  ``[P][n][n]`` float32 in the reference's centred layout);
+* :func:`mset_cuda_kernel` -- the reference's call signature
+  ``mset_cuda_kernel(mode, STEM_data, measured_cells)`` with MATLAB-shaped
+  arrays (``RVol`` of shape ``(n, n, nz)``, the measured cell array of shape
+  ``(N_scan_x, N_scan_y)``), one implicit session per process as the MEX keeps
+  one (mex_main.cu:13).
+
+Errors raise :class:`mset_b200._lib.MsetError`; nothing aborts.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any, Mapping, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import MSET_ADJOINT_EXACT, MSET_ADJOINT_REF, MSET_MODE_MSET, MSET_MODE_SSET, check, fptr
+
+_MODES = {"mset": MSET_MODE_MSET, "sset": MSET_MODE_SSET}
+
+
+def _c32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _cplx_f32(a) -> np.ndarray:
+    """complex array -> float32 [..., 2] interleaved view"""
+    z = np.ascontiguousarray(np.asarray(a, dtype=np.complex64))
+    return z.view(np.float32).reshape(z.shape + (2,))
+
+
+class Session:
+    """One device session: the state the MEX keeps between 'upload' and
+    'run_*' / 'error_*' calls, but with device buffers reused across uploads."""
+
+    def __init__(self, device: int = 0):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        check("mset_create", self._lib.mset_create(int(device), C.byref(h)))
+        self._h = h
+        self._keep: list = []
+        self.n = self.nz = self.npos = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.mset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- 'upload' (mex_main.cu:42-95) ----
+    def upload(self, rvol, probe, prop, *, sigma: float, potential_pixelsize: float,
+               scan_x, scan_y, measured, step_size=(0.0, 0.0, 0.0), slice_binning: int = 1,
+               n_scan_x: int | None = None, n_scan_y: int | None = None) -> None:
+        rvol = _c32(rvol)
+        if rvol.ndim != 3:
+            raise ValueError("rvol must be [nz][n][n]")
+        nz, n1, n2 = rvol.shape
+        if n1 != n2:
+            raise ValueError("only square windows are supported (the reference uses one centre, mset.cu:83)")
+        pr = _cplx_f32(probe)
+        pp = _cplx_f32(prop)
+        sx = _c32(scan_x).reshape(-1)
+        sy = _c32(scan_y).reshape(-1)
+        meas = _c32(measured).reshape(-1, n1, n1)
+        npos = sx.size
+        if sy.size != npos or meas.shape[0] != npos:
+            raise ValueError("scan_x, scan_y and measured must have one entry per position")
+        if pr.shape != (n1, n1, 2) or pp.shape != (n1, n1, 2):
+            raise ValueError("probe and prop must be n x n complex")
+        a = _lib.UploadArgs()
+        a.n, a.nz, a.num_scan_pos = n1, nz, npos
+        a.N_scan_x = int(n_scan_x if n_scan_x is not None else npos)
+        a.N_scan_y = int(n_scan_y if n_scan_y is not None else 1)
+        a.sigma = float(sigma)
+        a.potential_pixelsize = float(potential_pixelsize)
+        a.alpha = 0.0
+        a.E0 = 0.0
+        a.step_size[:] = [float(v) for v in step_size]
+        a.slice_binning = int(slice_binning)
+        a.RVol, a.init_wave2D, a.prop2D = fptr(rvol), fptr(pr), fptr(pp)
+        a.scan_xlist, a.scan_ylist, a.measured = fptr(sx), fptr(sy), fptr(meas)
+        self._keep = [rvol, pr, pp, sx, sy, meas]
+        check("mset_upload", self._lib.mset_upload(self._h, C.byref(a)))
+        self.n, self.nz, self.npos = n1, nz, npos
+
+    # ---- 'run_mset' / 'run_sset' (mex_main.cu:98-155) ----
+    def run(self, mode: int = MSET_MODE_MSET, adjoint: int = MSET_ADJOINT_REF, with_error: bool = True):
+        rv = np.empty((self.nz, self.n, self.n), np.float32)
+        pr = np.empty((self.n, self.n, 2), np.float32)
+        sx = np.empty(max(self.npos, 1), np.float32)
+        sy = np.empty(max(self.npos, 1), np.float32)
+        err = np.zeros(1, np.float32)
+        check("mset_run_ex", self._lib.mset_run_ex(self._h, int(mode), int(adjoint), fptr(rv), fptr(pr),
+                                                   fptr(sx), fptr(sy), fptr(err) if with_error else None))
+        probe = pr.view(np.complex64).reshape(self.n, self.n)
+        out = (rv, probe, sx[: self.npos].copy(), sy[: self.npos].copy())
+        return out + ((float(err[0]),) if with_error else ())
+
+    # ---- 'error_mset' / 'error_sset' (mex_main.cu:157-184) ----
+    def error(self, mode: int = MSET_MODE_MSET) -> float:
+        err = np.zeros(1, np.float32)
+        check("mset_error", self._lib.mset_error(self._h, int(mode), fptr(err)))
+        return float(err[0])
+
+
+# ---------------------------------------------------------------------------
+# reference call signature
+# ---------------------------------------------------------------------------
+_default: Session | None = None
+
+
+def _field(d: Mapping[str, Any], k: str):
+    if k not in d:
+        raise KeyError(f"STEM_data has no field '{k}'")
+    return d[k]
+
+
+def _scalar(v) -> float:
+    return float(np.asarray(v).reshape(-1)[0])
+
+
+def _cells_linear(cells) -> list:
+    """measured cell array -> list in MATLAB linear (column-major) order"""
+    if isinstance(cells, np.ndarray) and cells.dtype == object:
+        return list(cells.reshape(-1, order="F"))
+    if isinstance(cells, np.ndarray) and cells.ndim == 4:  # (nsx, nsy, n, n)
+        return [cells[i, j] for j in range(cells.shape[1]) for i in range(cells.shape[0])]
+    return list(cells)
+
+
+def mset_cuda_kernel(mode: str, STEM_data: Mapping[str, Any], measured_cells=None):
+    """Drop-in for the reference MEX function ``mset_cuda_kernel``
+    (mex_main.cu:19-39).
+
+    Arrays are MATLAB-shaped: ``RVol`` (n, n, nz), ``init_wave2D`` and
+    ``prop2D`` (n, n) complex, ``scan_xlist``/``scan_ylist`` (P,), the measured
+    cell array (N_scan_x, N_scan_y) of (n, n) patterns.  Returns what the MEX
+    returns: nothing for 'upload'; ``(RVol, probe, scan_x, scan_y[, error])``
+    for 'run_*' (the error is always returned here); ``error`` for 'error_*'.
+    """
+    global _default
+    if mode == "upload":
+        d = STEM_data
+        rvol_m = np.asarray(_field(d, "RVol"), dtype=np.float32)
+        rvol = np.ascontiguousarray(rvol_m.transpose(2, 1, 0))  # MATLAB (n,n,nz) -> C [nz][n][n]
+        probe = np.ascontiguousarray(np.asarray(_field(d, "init_wave2D")).T)
+        prop = np.ascontiguousarray(np.asarray(_field(d, "prop2D")).T)
+        cells = _cells_linear(measured_cells)
+        meas = np.stack([np.asarray(c, dtype=np.float32).T for c in cells]) if cells else \
+            np.zeros((0, rvol.shape[1], rvol.shape[2]), np.float32)
+        npos = int(_scalar(_field(d, "num_scan_pos")))
+        if _default is None:
+            _default = Session(0)
+        _default.upload(rvol, probe, prop, sigma=_scalar(_field(d, "sigma")),
+                        potential_pixelsize=_scalar(_field(d, "potential_pixelsize")),
+                        scan_x=np.asarray(_field(d, "scan_xlist")).reshape(-1)[:npos],
+                        scan_y=np.asarray(_field(d, "scan_ylist")).reshape(-1)[:npos],
+                        measured=meas[:npos],
+                        step_size=np.asarray(_field(d, "step_size"), dtype=np.float64).reshape(-1)[:3],
+                        slice_binning=int(_scalar(_field(d, "slice_binning"))),
+                        n_scan_x=int(_scalar(_field(d, "N_scan_x"))),
+                        n_scan_y=int(_scalar(_field(d, "N_scan_y"))))
+        return None
+    if mode in ("run_mset", "run_sset"):
+        if _default is None:
+            raise RuntimeError("run called before upload")
+        rv, pr, sx, sy, err = _default.run(_MODES[mode[4:]])
+        return rv.transpose(2, 1, 0), pr.T, sx, sy, err
+    if mode in ("error_mset", "error_sset"):
+        if _default is None:
+            raise RuntimeError("error called before upload")
+        return _default.error(_MODES[mode[6:]])
+    raise ValueError("The running mode is not correct (choose 'upload' or 'run_mset' or 'run_sset' "
+                     "or 'error_mset' or 'error_sset')")
+
+
+def clear() -> None:
+    """``clear mset_cuda_kernel`` (Run_MSET_recon.m:174): drop the session."""
+    global _default
+    if _default is not None:
+        _default.close()
+        _default = None
+
+
+__all__ = ["Session", "mset_cuda_kernel", "clear", "MSET_MODE_MSET", "MSET_MODE_SSET",
+           "MSET_ADJOINT_REF", "MSET_ADJOINT_EXACT"]

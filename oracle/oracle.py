@@ -1,0 +1,146 @@
+"""ctypes wrapper of oracle/libmset_oracle.so (FP64 restatement of the
+reference's per-position model and tilt passes, mset_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: the checker the CUDA library is compared against.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "libmset_oracle.so")
+_lib = None
+
+_F = C.POINTER(C.c_float)
+_D = C.POINTER(C.c_double)
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", HERE, "libmset_oracle.so"], check=True, capture_output=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "mset_oracle.c")):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_fft2.argtypes = [_D, C.c_int, C.c_int, C.c_int]
+        L.orc_run_tilt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _D, C.c_int, C.c_int,
+                                   C.c_int, C.c_int, _F, _F, _F, _F, _F, _F, _D]
+        L.orc_position.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _D, _D,
+                                   _D, C.c_double, C.c_double, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.orc_position_loss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _D, _D, _D,
+                                        C.c_double, C.c_double, _D]
+        L.orc_position_loss.restype = C.c_double
+        L.orc_batched_tilt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                       C.c_int, _F, _F, _F, _F, _F, _F, _D, _D, _D, _D, C.c_int]
+        L.orc_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return None if a is None else a.ctypes.data_as(_F)
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def fft2(a: np.ndarray, sign: int = -1) -> np.ndarray:
+    z = np.ascontiguousarray(a, dtype=np.complex128).copy()
+    lib().orc_fft2(z.view(np.float64).ctypes.data_as(_D), z.shape[0], z.shape[1], sign)
+    return z
+
+
+def run_tilt(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz, step=(0, 0, 0), binning=1,
+             method=1, adjoint=0, update=True):
+    """Sequential tilt pass (mset.cu run_main_* / run_error_*).  Returns
+    (rvol, probe, scan_x, scan_y, err_sum) with err_sum = sum over positions and
+    pixels of (A-M)^2 (not normalised)."""
+    rv = np.ascontiguousarray(rvol, dtype=np.float32).copy()
+    nz, n, _ = rv.shape
+    pr = np.ascontiguousarray(probe, dtype=np.complex64).copy()
+    pp = np.ascontiguousarray(prop, dtype=np.complex64)
+    sx = np.ascontiguousarray(scan_x, dtype=np.float32).copy()
+    sy = np.ascontiguousarray(scan_y, dtype=np.float32).copy()
+    me = np.ascontiguousarray(measured, dtype=np.float32)
+    st = np.asarray(step, dtype=np.float64)
+    err = np.zeros(1)
+    rc = lib().orc_run_tilt(n, nz, binning, sigma, dz, _d(st), method, adjoint, int(update), sx.size,
+                            _f(rv), pr.view(np.float32).ctypes.data_as(_F), pp.view(np.float32).ctypes.data_as(_F),
+                            _f(sx), _f(sy), _f(me), _d(err))
+    assert rc == 0
+    return rv, pr, sx, sy, float(err[0])
+
+
+def amp_std(measured_one: np.ndarray) -> np.ndarray:
+    """sqrt(ifftshift(I)) in standard FFT order (mset.cu:206-210)."""
+    return np.ascontiguousarray(np.sqrt(np.fft.ifftshift(np.asarray(measured_one, dtype=np.float64))))
+
+
+def position(V, probe, prop, scan_x, scan_y, amp, *, sigma, dz, binning=1, method=1, adjoint=0):
+    """One position in FP64: dict with psi0, far, err, grad (ns slabs, complex),
+    chi0, probe_dir, pos_dir."""
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    nz, n, _ = V.shape
+    ns = 1 if method == 2 else -(-nz // binning)
+    pr = np.ascontiguousarray(probe, dtype=np.complex128)
+    pp = np.ascontiguousarray(prop, dtype=np.complex128)
+    am = np.ascontiguousarray(amp, dtype=np.float64)
+    out = dict(psi0=np.zeros((n, n), np.complex128), far=np.zeros((n, n), np.complex128),
+               grad=np.zeros((ns, n, n), np.complex128), chi0=np.zeros((n, n), np.complex128),
+               probe_dir=np.zeros((n, n), np.complex128))
+    err = np.zeros(1)
+    pd = np.zeros(2)
+    c = lambda a: a.view(np.float64).ctypes.data_as(_D)
+    rc = lib().orc_position(n, nz, binning, sigma, dz, method, adjoint, _d(V), c(pr), c(pp), float(scan_x),
+                            float(scan_y), _d(am), c(out["psi0"]), c(out["far"]), _d(err), c(out["grad"]),
+                            c(out["chi0"]), c(out["probe_dir"]), _d(pd))
+    assert rc == 0
+    out["err"] = float(err[0])
+    out["pos_dir"] = pd
+    return out
+
+
+def position_loss(V, probe, prop, scan_x, scan_y, amp, *, sigma, dz, binning=1, method=1) -> float:
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    nz, n, _ = V.shape
+    pr = np.ascontiguousarray(probe, dtype=np.complex128)
+    pp = np.ascontiguousarray(prop, dtype=np.complex128)
+    am = np.ascontiguousarray(amp, dtype=np.float64)
+    c = lambda a: a.view(np.float64).ctypes.data_as(_D)
+    return lib().orc_position_loss(n, nz, binning, sigma, dz, method, _d(V), c(pr), c(pp), float(scan_x),
+                                   float(scan_y), _d(am))
+
+
+def batched_tilt(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz, binning=1, method=1, adjoint=0,
+                 nthreads=0):
+    """Batched pass over one tilt: (grad_slab [ns][n][n], probe_acc [n][n]
+    complex, pos_dir [P][2], err_sum)."""
+    rv = np.ascontiguousarray(rvol, dtype=np.float32)
+    nz, n, _ = rv.shape
+    ns = 1 if method == 2 else -(-nz // binning)
+    pr = np.ascontiguousarray(probe, dtype=np.complex64)
+    pp = np.ascontiguousarray(prop, dtype=np.complex64)
+    sx = np.ascontiguousarray(scan_x, dtype=np.float32)
+    sy = np.ascontiguousarray(scan_y, dtype=np.float32)
+    me = np.ascontiguousarray(measured, dtype=np.float32)
+    g = np.zeros((ns, n, n))
+    pa = np.zeros((n, n, 2))
+    pd = np.zeros((sx.size, 2))
+    err = np.zeros(1)
+    rc = lib().orc_batched_tilt(n, nz, binning, sigma, dz, method, adjoint, sx.size, _f(rv),
+                                pr.view(np.float32).ctypes.data_as(_F), pp.view(np.float32).ctypes.data_as(_F),
+                                _f(sx), _f(sy), _f(me), _d(g), _d(pa), _d(pd), _d(err), int(nthreads))
+    assert rc == 0
+    return g, pa[..., 0] + 1j * pa[..., 1], pd, float(err[0])
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()

@@ -1,0 +1,143 @@
+"""GPU parity: libmset_b200.so (through the C ABI) against the FP64 oracle on
+the same seeded inputs.  Tolerance: relative L2 <= 1e-4 (FP32 propagation
+against FP64), stated per assertion.
+
+Sequential mode compares the *changes* the pass makes (RVol_out - RVol_in,
+probe_out - probe_in, positions_out - positions_in), which is what the
+reference's run_mset computes; the unchanged part of RVol would hide errors.
+"""
+import numpy as np
+import pytest
+
+from mset_b200 import MSET_ADJOINT_EXACT, MSET_ADJOINT_REF, MSET_MODE_MSET, MSET_MODE_SSET, Session
+from mset_b200.batch import BatchSession
+from oracle import oracle as O
+from tests.helpers import reasonable_steps, rel_l2, small_case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+STRENGTH = 20.0  # object strength: phase ~0.1-0.3 rad, so every gradient carries signal
+
+
+def pos_tol(n: int) -> float:
+    """Scan-position directions are sums over N^2 products with cancellation
+    factors sum|t|/|sum t| of ~1e3; FP32 propagation limits them to ~1e-4 at
+    N <= 96 and ~4e-4 at N = 160.  On the same inputs the reference's own FP32
+    CUDA code (float host sums, utility.cu:928-942) deviates from the FP64
+    oracle by 2-3x more (measured 2.7e-4 at N = 128, 9.5e-4 at N = 160)."""
+    return TOL if n <= 96 else 5e-4
+
+
+def _steps(c, method, admode=0):
+    return reasonable_steps(c, method, admode)
+
+
+CASES = [
+    dict(n=64, nz=8, npos=6, b=1),
+    dict(n=64, nz=9, npos=5, b=2),
+    dict(n=24, nz=6, npos=7, b=1),
+    dict(n=128, nz=4, npos=3, b=2),
+    dict(n=96, nz=3, npos=3, b=1),
+    dict(n=160, nz=3, npos=2, b=1),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"n{c['n']}z{c['nz']}b{c['b']}")
+@pytest.mark.parametrize("method", [MSET_MODE_MSET, MSET_MODE_SSET], ids=["mset", "sset"])
+def test_sequential_run_matches_oracle(gpu_available, case, method):
+    c = small_case(n=case["n"], nz=case["nz"], npos=case["npos"], b=case["b"], seed=case["n"] + case["nz"],
+                   defocus=20.0, jitter=4.0, strength=STRENGTH)
+    step = _steps(c, method)
+    rv_o, pr_o, sx_o, sy_o, err_o = O.run_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"],
+                                               sigma=c["sigma"], dz=c["dz"], step=step, binning=c["b"],
+                                               method=method)
+    with Session() as s:
+        s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"], scan_x=c["sx"],
+                 scan_y=c["sy"], measured=c["meas"], step_size=step, slice_binning=c["b"],
+                 n_scan_x=case["npos"], n_scan_y=1)
+        rv, pr, sx, sy, err = s.run(method)
+    n2 = case["n"] ** 2
+    assert rel_l2(rv - c["V"], rv_o - c["V"]) < TOL
+    assert rel_l2(pr - c["probe"], pr_o - c["probe"]) < TOL
+    assert rel_l2(np.r_[sx - c["sx"], sy - c["sy"]], np.r_[sx_o - c["sx"], sy_o - c["sy"]]) < pos_tol(case["n"])
+    assert abs(err - err_o / case["npos"] / n2) <= TOL * abs(err_o / case["npos"] / n2)
+
+
+@pytest.mark.parametrize("method", [MSET_MODE_MSET, MSET_MODE_SSET], ids=["mset", "sset"])
+def test_error_pass_matches_oracle(gpu_available, method):
+    c = small_case(n=64, nz=7, npos=9, b=2, seed=4, defocus=10.0, jitter=5.0)
+    _, _, _, _, err_o = O.run_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"], sigma=c["sigma"],
+                                   dz=c["dz"], binning=c["b"], method=method, update=False)
+    with Session() as s:
+        s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"], scan_x=c["sx"],
+                 scan_y=c["sy"], measured=c["meas"], slice_binning=c["b"], n_scan_x=3, n_scan_y=3)
+        e = s.error(method)
+    ref = err_o / 9 / 64 ** 2  # mex_main.cu:179
+    assert abs(e - ref) <= TOL * ref
+
+
+@pytest.mark.parametrize("admode", [MSET_ADJOINT_REF, MSET_ADJOINT_EXACT], ids=["ref", "exact"])
+@pytest.mark.parametrize("method", [MSET_MODE_MSET, MSET_MODE_SSET], ids=["mset", "sset"])
+@pytest.mark.parametrize("n", [64, 128])
+def test_batched_gradient_matches_oracle(gpu_available, admode, method, n):
+    tilts = [small_case(n=n, nz=6, npos=5, b=2, seed=20 + j, defocus=15.0, jitter=6.0, strength=STRENGTH)
+             for j in range(2)]
+    c0 = tilts[0]
+    bs = BatchSession(n=n, nz=6, npos=[5, 5], prop=c0["prop"], sigma=c0["sigma"], potential_pixelsize=c0["dz"],
+                      slice_binning=2, method=method, adjoint=admode)
+    for j, c in enumerate(tilts):
+        bs.set_tilt(j, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"], volume=c["V"])
+    out = bs.gradient()
+    bs.close()
+    for j, c in enumerate(tilts):
+        g, pa, pd, e = O.batched_tilt(c["V"], c["probe"], c0["prop"], c["sx"], c["sy"], c["meas"],
+                                      sigma=c0["sigma"], dz=c0["dz"], binning=2, method=method, adjoint=admode)
+        assert rel_l2(out["grad"][j], g) < TOL
+        assert rel_l2(np.fft.fft2(out["probe"][j]), pa) < TOL
+        assert rel_l2(out["posdir"][5 * j:5 * j + 5], pd) < (TOL if n <= 96 else 3e-4)
+        assert abs(out["err"][j] - e) <= TOL * e
+
+
+def test_simulate_matches_oracle_far_field(gpu_available):
+    c = small_case(n=64, nz=5, npos=4, b=1, seed=9, defocus=30.0, jitter=8.0)
+    bs = BatchSession(n=64, nz=5, npos=[4], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+    bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"], volume=c["V"])
+    I = bs.simulate()
+    bs.close()
+    for p in range(4):
+        o = O.position(c["V"], c["probe"], c["prop"], c["sx"][p], c["sy"][p], O.amp_std(c["meas"][p]),
+                       sigma=c["sigma"], dz=c["dz"])
+        ref = np.fft.fftshift(np.abs(o["far"]) ** 2)  # centred layout
+        assert rel_l2(I[p], ref) < TOL
+
+
+def test_unsupported_window_is_an_error(gpu_available):
+    import mset_b200
+    c = small_case(n=20, nz=2, npos=1)
+    with Session() as s:
+        with pytest.raises(mset_b200.MsetError, match="window size 20"):
+            s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"],
+                     scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"])
+
+
+def test_mex_signature_roundtrip(gpu_available):
+    """mset_cuda_kernel with MATLAB-shaped arrays equals the Session path"""
+    import mset_b200
+    c = small_case(n=24, nz=4, npos=4, b=1, seed=2, defocus=10.0, jitter=3.0)
+    step = _steps(c, 1)
+    cells = np.empty((2, 2), dtype=object)
+    for k in range(4):
+        cells[k % 2, k // 2] = c["meas"][k].T  # MATLAB (n, n) pattern, column-major cell
+    STEM = dict(RVol=c["V"].transpose(2, 1, 0), init_wave2D=c["probe"].T, prop2D=c["prop"].T, alpha=20.0,
+                sigma=c["sigma"], E0=300.0, potential_pixelsize=c["dz"], N_scan_x=2, N_scan_y=2,
+                scan_xlist=c["sx"], scan_ylist=c["sy"], num_scan_pos=4, step_size=np.array(step), slice_binning=1)
+    mset_b200.mset_cuda_kernel("upload", STEM, cells)
+    rvm, prm, sxm, sym, errm = mset_b200.mset_cuda_kernel("run_mset", STEM, cells)
+    mset_b200.clear()
+    with Session() as s:
+        s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"], scan_x=c["sx"],
+                 scan_y=c["sy"], measured=c["meas"], step_size=step, n_scan_x=2, n_scan_y=2)
+        rv, pr, sx, sy, err = s.run(1)
+    np.testing.assert_array_equal(rvm.transpose(2, 1, 0), rv)
+    np.testing.assert_array_equal(prm.T, pr)
+    assert errm == err
