@@ -50,6 +50,9 @@ CONFIGS = {
     # batched mid-size: 128^3 at 0.3 A, 128^2 window, 32x32 scan at 3 px,
     # 21 tilts over +-60 deg, 64 slices of 2 voxels
     "mid": Config("mid", (128, 128, 128), 0.3, 128, (32, 32), 3.0, 21, 60.0, 2, 1e4),
+    # the mid-size geometry (128^2 window, 64 slabs of 2 voxels) on a small
+    # position set: 2 tilts x 8x8 scan, for profiling captures
+    "mid_s": Config("mid_s", (128, 128, 128), 0.3, 128, (8, 8), 3.0, 2, 60.0, 2, 1e4),
     # adjoint / gradient validation: the small sample in a 128^2 window with
     # +-5 nm defocus and C3 = 1 mm +- 1 um probe errors and +-0.5 px jitter
     "grad": Config("grad", (24, 24, 24), 0.4, 128, (12, 12), 2.0, 5, 30.0, 1, 1e4,
