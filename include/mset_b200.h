@@ -159,6 +159,36 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 
+/* ---- allocation-free batched pass -------------------------------------------
+ * Has no counterpart in the reference.  For callers that cannot allocate
+ * device memory (work issued while a CUDA graph is being captured, device
+ * memory owned by a framework allocator or by MATLAB gpuArrays, real-time
+ * pipelines that forbid allocation after start-up): one batched forward +
+ * adjoint pass over the npos positions of ONE tilt, every input and output a
+ * caller-owned DEVICE pointer, no cudaMalloc / cudaFree or allocating library
+ * call.  Its scratch (saved waves, prepared propagator and probe spectrum,
+ * probe accumulator, work counter) is a fixed 64 MiB device array inside the
+ * library, held by every GPU that loads the library until the process exits.
+ *   n in {24, 64, 128}; 0 < npos <= 131072; sizes whose (ns + 1) saved waves
+ *   of n x n complex64 do not fit beside the fixed part of the 64 MiB are
+ *   rejected with MSET_E_UNSUPPORTED (n = 128 allows ns up to ~500).
+ * Inputs (device): rvol [nz][n][n] float, probe [n][n][2] float, prop2D
+ * [n][n][2] centred, scan_x/scan_y [npos], measured [npos][n][n] centred
+ * intensities.  Outputs (device), all overwritten: grad [ns][n][n] double,
+ * probe_out [n][n][2] double (standard FFT order), posdir [npos][2] double,
+ * err [1] double -- the same quantities mset_batch_gradient returns.
+ * Work is queued on `stream` (a cudaStream_t, NULL = legacy default stream)
+ * and is asynchronous.  The first call on a device resolves the scratch
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Every call shares the scratch array, so calls whose
+ * work overlaps on the GPU (other streams, other host threads) race: order
+ * them on one stream. */
+int mset_batch_gradient_noalloc(int device, void *stream, int n, int nz, int slice_binning, int method,
+                                int adjoint, float sigma, float potential_pixelsize, int npos,
+                                const float *rvol_dev, const float *probe_dev, const float *prop2D_dev,
+                                const float *scan_x_dev, const float *scan_y_dev, const float *measured_dev,
+                                double *grad_dev, double *probe_out_dev, double *posdir_dev, double *err_dev);
+
 #ifdef __cplusplus
 }
 #endif

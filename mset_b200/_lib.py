@@ -50,6 +50,8 @@ SIGNATURES = {
     "mset_batch_get_tilt": (C.c_int, [C.c_void_p, C.c_int, _F, _F, _F, _F]),
     "mset_batch_time": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "mset_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "mset_batch_gradient_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              C.c_float, C.c_float, C.c_int] + [C.c_void_p] * 10),
 }
 
 

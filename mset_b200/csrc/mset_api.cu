@@ -65,6 +65,10 @@ struct DevBuf {
 
 }  // namespace
 
+namespace mset {
+void set_last_error(const char *msg) { g_err = msg; }
+}  // namespace mset
+
 struct TiltBufs {
     DevBuf<float> V;
     DevBuf<float2> Q;

@@ -13,14 +13,15 @@ enum Mode {
     kSeq = 0,    // reference semantics: update volume, probe and position after every position
     kBatch = 1,  // fixed state, accumulate FP64 gradients over positions
     kErr = 2,    // forward + error only (run_error_mset / run_error_sset)
-    kSim = 3     // forward + write |Psi|^2 (centred layout)
+    kSim = 3,    // forward + write |Psi|^2 (centred layout)
+    kBatchCentred = 4  // kBatch reading the caller's centred intensities (no prepared amplitudes)
 };
 
 // one tilt: all buffers on the device
 struct TiltDev {
     float *V;            // [nz][n][n] beam-frame potential (kSeq: updated in place)
     float2 *Q;           // [n][n] scrambled F^{-1}(probe)  (kSeq: updated in place)
-    const float *amp;    // [npos][n][n] scrambled sqrt(ifftshift(I_meas))
+    const float *amp;    // [npos][n][n] scrambled sqrt(ifftshift(I_meas)); kBatchCentred: centred I_meas
     float *sx, *sy;      // [npos] 1-based scan coordinates (kSeq: updated in place)
     double *grad;        // kBatch: [ns][n][n] sum_p Re(g)   (natural layout)
     double *qacc;        // kBatch: [n][n][2] scrambled sum_p F^{-1}(chi0) fs(-s)
@@ -70,6 +71,9 @@ int launch_prep_amp(const Plan &pl, const float *meas_centred, float *amp_scr, l
 int launch_prep_prop(const Plan &pl, const float *prop_centred, float2 *pscr, cudaStream_t st);
 int launch_probe_to_q(const Plan &pl, const float2 *probe, float2 *q, const float2 *twn, cudaStream_t st);
 int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const float2 *twn, cudaStream_t st);
+// thread-local error message of the C ABI (mset_last_error)
+void set_last_error(const char *msg);
+
 int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,
                        const TiltDev *tilts_host, int ntilts, cudaStream_t st);
 

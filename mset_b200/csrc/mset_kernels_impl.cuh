@@ -84,6 +84,20 @@ struct PositionKernel {
         return make_float2(cs, sn);
     }
 
+    // measured amplitude at scrambled location (Ly, Lx): prepared sqrt(I) in
+    // scrambled layout, or (kBatchCentred) gathered from the centred pattern
+    static __device__ __forceinline__ float meas_amp(const float *amp, int Ly, int Lx) {
+        if constexpr (MODE == kBatchCentred) {
+            const int h = (N + 1) / 2;
+            int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+            if (r < 0) r += N;
+            if (c < 0) c += N;
+            return sqrtf(__ldg(amp + (size_t)r * N + c));
+        } else {
+            return __ldg(amp + (size_t)Ly * N + Lx);
+        }
+    }
+
     static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, const float2 *tw,
                                float2 *e1, float2 *e2, double *red, float2 *save) {
         const int ns = METHOD == kSSET ? 1 : a.ns;
@@ -184,7 +198,7 @@ struct PositionKernel {
                         t.inten[(size_t)p * NN + (size_t)r * N + c] = a2;
                     } else {
                         const float A = sqrtf(a2 + 1e-30f);
-                        const float M = __ldg(amp + (size_t)(y0 + j) * N + x);
+                        const float M = meas_amp(amp, y0 + j, x);
                         const float d = A - M;
                         err += (double)(d * d);
                     }
@@ -204,7 +218,7 @@ struct PositionKernel {
                 for (int j = 0; j < G::R1; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     const float A = sqrtf(a2 + 1e-30f);
-                    const float M = __ldg(amp + (size_t)(y0 + j) * N + x);
+                    const float M = meas_amp(amp, y0 + j, x);
                     const float d = A - M;
                     err += (double)(d * d);
                     float2 r = cscale(v[j], 1.0f - M / A);
