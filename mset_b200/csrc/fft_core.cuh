@@ -21,7 +21,8 @@
 // rows.  The passes that border a pointwise stage are fused with it:
 //   row pass A  = [inverse rows A] + op(real space, natural order) + [forward rows A]
 //   col pass B  = [forward cols B] + op(Fourier space, scrambled)   + [inverse cols B]
-// so one propagation slab costs six shared-memory round trips.
+// so one propagation slab costs six shared-memory round trips, with a
+// CTA-wide barrier only where row passes meet column passes.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -243,16 +244,52 @@ __device__ __forceinline__ float2 twN(const float2 *tw, int n1, int k2) {
     return SG < 0 ? w : cconj(w);
 }
 
+// Work ownership.  Row passes: warp w owns rows [w*RPW, (w+1)*RPW), so the
+// two row passes of a transform only need __syncwarp between them.  Column
+// passes: warp pair q owns columns [q*CPP, (q+1)*CPP), a named barrier of the
+// pair separates them.  Only a switch between row and column passes needs
+// the CTA-wide barrier; warps drift apart inside each phase, so one warp's
+// global-memory latency overlaps another warp's arithmetic.
+template <class G>
+struct Own {
+    static constexpr int W = G::NT / 32;           // warps
+    static constexpr int RPW = G::N / W;            // rows per warp
+    static constexpr int CPP = 2 * G::N / W;        // columns per warp pair
+    static_assert(G::NT % 64 == 0, "NT must be a multiple of 64");
+    static_assert(G::N % W == 0 && (2 * G::N) % W == 0, "rows must split evenly over warps");
+    __device__ __forceinline__ static int warp() { return threadIdx.x >> 5; }
+    __device__ __forceinline__ static int lane() { return threadIdx.x & 31; }
+    __device__ __forceinline__ static int pair() { return threadIdx.x >> 6; }
+    __device__ __forceinline__ static int plane() { return threadIdx.x & 63; }
+};
+
+__device__ __forceinline__ void sync_rows() { __syncwarp(); }
+template <class G>
+__device__ __forceinline__ void sync_cols() {
+    // named barrier per warp pair (ids 1..15; 0 is __syncthreads)
+    asm volatile("bar.sync %0, 64;" ::"r"(1 + Own<G>::pair()) : "memory");
+}
+__device__ __forceinline__ void sync_all() { __syncthreads(); }
+
+struct NoPre {};
+
 // Row pass A.  Task (y, n1) owns x = n1 + R1*j, j < R2.
+//   pf(y, n1, pre) : issue the global loads the op needs (before the shared
+//                    memory reads, so their latency overlaps them)
 //   IN  != 0 : finish a scrambled->natural transform of sign IN
-//   op(y, n1, v) : pointwise stage on natural-order real-space values
+//   op(y, n1, v, pre) : pointwise stage on natural-order real-space values
 //   OUT != 0 : start a natural->scrambled transform of sign OUT
-template <class G, int IN, int OUT, class Op>
-__device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op) {
+template <class G, int IN, int OUT, class Pre, class Pf, class Op>
+__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op) {
+    using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
+    constexpr int TASKS = O::RPW * R1;
+    const int y0 = O::warp() * O::RPW;
 #pragma unroll 1
-    for (int t = threadIdx.x; t < G::NRA; t += G::NT) {
-        const int n1 = t % R1, y = t / R1;
+    for (int tau = O::lane(); tau < TASKS; tau += 32) {
+        const int n1 = tau % R1, y = y0 + tau / R1;
+        Pre pre;
+        pf(y, n1, pre);
         float2 *row = buf + y * G::S + n1;
         float2 v[R2];
 #pragma unroll
@@ -262,7 +299,7 @@ __device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op
             for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, IN>(tw, n1, k2));
             DFT<R2, IN>::run(v);
         }
-        op(y, n1, v);
+        op(y, n1, v, pre);
         if constexpr (OUT != 0) {
             DFT<R2, OUT>::run(v);
 #pragma unroll
@@ -273,13 +310,22 @@ __device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op
     }
 }
 
+template <class G, int IN, int OUT, class Op>
+__device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op) {
+    row_passA_pf<G, IN, OUT, NoPre>(
+        buf, tw, [](int, int, NoPre &) {}, [&](int y, int n1, float2 *v, const NoPre &) { op(y, n1, v); });
+}
+
 // Row pass B.  Task (y, k2) owns x = j + R1*k2, j < R1.
 template <class G, int SG>
 __device__ __forceinline__ void row_passB(float2 *buf) {
+    using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
+    constexpr int TASKS = O::RPW * R2;
+    const int y0 = O::warp() * O::RPW;
 #pragma unroll 1
-    for (int t = threadIdx.x; t < G::NRB; t += G::NT) {
-        const int k2 = t % R2, y = t / R2;
+    for (int tau = O::lane(); tau < TASKS; tau += 32) {
+        const int k2 = tau % R2, y = y0 + tau / R2;
         float2 *p = buf + y * G::S + (R1 + 1) * k2;
         float2 v[R1];
 #pragma unroll
@@ -294,10 +340,13 @@ __device__ __forceinline__ void row_passB(float2 *buf) {
 //   FWD: natural->scrambled step (DFT then twiddle); else scrambled->natural
 template <class G, int SG, bool FWD>
 __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
+    using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
+    constexpr int TASKS = O::CPP * R1;
+    const int x0 = O::pair() * O::CPP;
 #pragma unroll 1
-    for (int t = threadIdx.x; t < G::NRA; t += G::NT) {
-        const int x = t % G::N, n1 = t / G::N;
+    for (int tau = O::plane(); tau < TASKS; tau += 64) {
+        const int x = x0 + tau % O::CPP, n1 = tau / O::CPP;
         float2 *p = buf + n1 * G::S + G::px(x);
         float2 v[R2];
 #pragma unroll
@@ -322,10 +371,13 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
 //   OUT != 0 : start scrambled->natural (sign OUT)
 template <class G, int IN, int OUT, class Op>
 __device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
-    constexpr int R1 = G::R1;
+    using O = Own<G>;
+    constexpr int R1 = G::R1, R2 = G::R2;
+    constexpr int TASKS = O::CPP * R2;
+    const int x0 = O::pair() * O::CPP;
 #pragma unroll 1
-    for (int t = threadIdx.x; t < G::NRB; t += G::NT) {
-        const int x = t % G::N, k2 = t / G::N;
+    for (int tau = O::plane(); tau < TASKS; tau += 64) {
+        const int x = x0 + tau % O::CPP, k2 = tau / O::CPP;
         const int y0 = R1 * k2;
         float2 *p = buf + y0 * G::S + G::px(x);
         float2 v[R1];

@@ -1,5 +1,6 @@
 // mset_api.cu -- C ABI (include/mset_b200.h): sessions, validation, device
 // buffers, the MEX-compatible modes and the batched method.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -70,6 +71,7 @@ void set_last_error(const char *msg) { g_err = msg; }
 }  // namespace mset
 
 struct TiltBufs {
+    DevBuf<float2> T;  // batched method: precomputed transmission slabs
     DevBuf<float> V;
     DevBuf<float2> Q;
     DevBuf<float> amp;
@@ -96,7 +98,8 @@ struct mset_session {
     std::vector<int> pos_off;
     int total_pos = 0;
     // shared buffers
-    DevBuf<float2> pscr, twn, save, tmpc;
+    DevBuf<float2> pscr, psep, twn, save, tmpc;
+    bool sep = false;  // propagator is numerically separable: P = Py (x) Px
     DevBuf<float> meas_tmp;
     DevBuf<double> err;
     DevBuf<TiltDev> d_tilts;
@@ -152,6 +155,46 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
     // propagator: host centred -> device -> scrambled / N^2
     CK(cudaMemcpyAsync(s->tmpc.p, prop, sizeof(float2) * n2, cudaMemcpyHostToDevice, s->st));
     CKL(launch_prep_prop(pl, reinterpret_cast<const float *>(s->tmpc.p), s->pscr.p, s->st), "prep_prop");
+    // The Fresnel propagator exp(-i pi lambda dz (qx^2 + qy^2)) is a product
+    // Py(ky) Px(kx) (Func_generate_propagator.m:36); when the caller's table
+    // is separable to FP32 rounding, the kernels keep the two vectors in
+    // shared memory instead of reading the n x n table.
+    {
+        const int h = (n + 1) / 2, r1 = pl.r1, r2 = n / r1;
+        std::vector<double> re(n2), im(n2);
+        double mx = 0;
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) {
+                const size_t o = (size_t)((r + h) % n) * n + (c + h) % n;
+                re[o] = prop[2 * ((size_t)r * n + c)];
+                im[o] = prop[2 * ((size_t)r * n + c) + 1];
+                mx = std::max(mx, std::hypot(re[o], im[o]));
+            }
+        const double a0 = re[0], b0 = im[0], d0 = a0 * a0 + b0 * b0;
+        s->sep = d0 > 1e-6 * mx * mx;
+        double e = 0;
+        for (int ky = 0; ky < n && s->sep; ++ky)
+            for (int kx = 0; kx < n; ++kx) {
+                // u[ky] v[kx] with u = P[:, 0], v = P[0, :] / P[0][0]
+                const double ur = re[(size_t)ky * n], ui = im[(size_t)ky * n];
+                const double vr = (re[kx] * a0 + im[kx] * b0) / d0, vi = (im[kx] * a0 - re[kx] * b0) / d0;
+                const double pr = ur * vr - ui * vi, pi = ur * vi + ui * vr;
+                e = std::max(e, std::hypot(pr - re[(size_t)ky * n + kx], pi - im[(size_t)ky * n + kx]));
+            }
+        s->sep = s->sep && e <= 2e-6 * mx;
+        if (s->sep) {
+            std::vector<float2> h2(2 * n);
+            for (int L = 0; L < n; ++L) {
+                const int k = L / r1 + r2 * (L % r1);
+                h2[L] = make_float2((float)(re[(size_t)k * n] / n), (float)(im[(size_t)k * n] / n));
+                const double vr = (re[k] * a0 + im[k] * b0) / d0, vi = (im[k] * a0 - re[k] * b0) / d0;
+                h2[n + L] = make_float2((float)(vr / n), (float)(vi / n));
+            }
+            CK(s->psep.ensure(2 * n));
+            CK(cudaMemcpyAsync(s->psep.p, h2.data(), sizeof(float2) * 2 * n, cudaMemcpyHostToDevice, s->st));
+            CK(cudaStreamSynchronize(s->st));
+        }
+    }
     CK(s->err.ensure(64));
     CK(s->counter.ensure(1));
     return 0;
@@ -201,6 +244,7 @@ int refresh_tilt_table(mset_session *s) {
         d.posdir = t.posdir.p;
         d.err = s->err.p + j;
         d.inten = s->inten.p ? s->inten.p + (size_t)s->pos_off[j] * s->n * s->n : nullptr;
+        d.T = s->batch ? t.T.p : nullptr;
         d.npos = t.npos;
     }
     CK(s->d_tilts.ensure(J));
@@ -226,6 +270,7 @@ LaunchArgs base_args(mset_session *s) {
     a.counter = s->counter.p;
     a.save = s->save.p;
     a.pscr = s->pscr.p;
+    a.psep = s->sep ? s->psep.p : nullptr;
     a.twn = s->twn.p;
     a.nz = s->nz;
     a.b = s->b;
@@ -441,6 +486,7 @@ int mset_batch_setup(mset_session *s, const mset_batch_args *a) {
     if (rc) return rc;
     s->method = a->method;
     s->adjoint = a->adjoint;
+    s->batch = true;
     for (int i = 0; i < 3; ++i) s->step[i] = a->step_size[i];
     s->nsx = s->nsy = 1;
     const int J = a->ntilts;
@@ -458,6 +504,7 @@ int mset_batch_setup(mset_session *s, const mset_batch_args *a) {
         TiltBufs &t = s->tilts[j];
         t.npos = a->npos[j];
         CK(t.V.ensure(n2 * s->nz));
+        CK(t.T.ensure(n2 * nsg));
         CK(t.Q.ensure(n2));
         CK(t.amp.ensure(n2 * t.npos));
         CK(t.sx.ensure(std::max(1, t.npos)));
@@ -530,10 +577,23 @@ static int batch_zero(mset_session *s) {
     return 0;
 }
 
+// transmission slabs of every tilt from the current volumes
+static int batch_transmission(mset_session *s) {
+    int rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
+    const int b = s->method == MSET_MODE_SSET ? s->nz : s->b;
+    CKL(launch_transmission(s->d_tilts.p, (int)s->tilts.size(), s->n, s->nz, b, nsg, s->sigma * s->dz, s->st),
+        "transmission");
+    return 0;
+}
+
 static int batch_pass(mset_session *s) {
     int rc = batch_zero(s);
     if (rc) return rc;
     if (s->total_pos == 0) return 0;
+    rc = batch_transmission(s);
+    if (rc) return rc;
     return launch_queue(s, s->method, s->adjoint, kBatch);
 }
 
@@ -578,6 +638,8 @@ int mset_batch_error(mset_session *s, double *err_out) {
     if (rc) return rc;
     CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * s->tilts.size(), s->st));
     if (s->total_pos) {
+        rc = batch_transmission(s);
+        if (rc) return rc;
         rc = launch_queue(s, s->method, kREF, kErr);
         if (rc) return rc;
     }
@@ -593,6 +655,8 @@ int mset_batch_simulate(mset_session *s, float *inten_out) {
     const size_t n2 = (size_t)s->n * s->n;
     CK(s->inten.ensure(std::max<size_t>(1, n2 * s->total_pos)));
     if (s->total_pos) {
+        rc = batch_transmission(s);
+        if (rc) return rc;
         rc = launch_queue(s, s->method, kREF, kSim);
         if (rc) return rc;
         CK(cudaMemcpyAsync(inten_out, s->inten.p, sizeof(float) * n2 * s->total_pos, cudaMemcpyDeviceToHost, s->st));
@@ -650,7 +714,7 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
 
 int mset_batch_launch_count(mset_session *s) {
     if (!s) return fail(MSET_E_ARG, "null session");
-    return 1;
+    return 2;  // transmission slabs + position kernel
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include "mset_kernels.cuh"
 
+
 namespace mset {
 
 #define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(96) X(128) X(160)
@@ -71,6 +72,34 @@ __global__ void k_apply_pos(float *sx, float *sy, const double *pd, int npos, fl
         sx[i] += step2 * (float)pd[2 * i];
         sy[i] += step2 * (float)pd[2 * i + 1];
     }
+}
+
+// transmission slabs of every tilt: T[s][y][x] = exp(i sdz sum_{z in slab s} V)
+// (mset.cu:134-153), once per pass so the position kernel reads one complex
+// value instead of recomputing it in the forward and the adjoint
+__global__ void k_transmission(const TiltDev *tilts, int ntilts, int n2, int nz, int b, int ns, float sdz) {
+    const long per = (long)ns * n2;
+    const long total = per * ntilts;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / per);
+        const long r = i % per;
+        const int s = (int)(r / n2);
+        const int l = (int)(r % n2);
+        const TiltDev &t = tilts[j];
+        const int z0 = s * b, z1 = min(z0 + b, nz);
+        float acc = 0.f;
+        for (int z = z0; z < z1; ++z) acc += __ldg(t.V + (size_t)z * n2 + l);
+        float sn, cs;
+        sincosf(sdz * acc, &sn, &cs);
+        const_cast<float2 *>(t.T)[r] = make_float2(cs, sn);
+    }
+}
+
+int launch_transmission(const TiltDev *tilts, int ntilts, int n, int nz, int b, int ns, float sdz, cudaStream_t st) {
+    const long total = (long)ntilts * ns * n * n;
+    const int grid = (int)std::min<long>((total + 255) / 256, 148L * 16);
+    k_transmission<<<grid, 256, 0, st>>>(tilts, ntilts, n * n, nz, b, ns, sdz);
+    return (int)cudaGetLastError();
 }
 
 int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,

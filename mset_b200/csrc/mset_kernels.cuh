@@ -28,6 +28,7 @@ struct TiltDev {
     double *posdir;      // kBatch: [npos][2]
     double *err;         // [1] sum over positions and pixels of (A-M)^2
     float *inten;        // kSim: [npos][n][n] centred |Psi|^2
+    const float2 *T;     // [ns][n][n] precomputed transmission slabs, or null (computed from V)
     int npos;
     int pad_;
 };
@@ -39,6 +40,7 @@ struct LaunchArgs {
     unsigned *counter;      // work-queue counter (zeroed before the launch)
     float2 *save;           // per-CTA saved waves: [grid][ns+1][n][n]
     const float2 *pscr;     // propagator / N^2, scrambled layout
+    const float2 *psep;     // separable propagator: [2n] = (Py / N, Px / N) scrambled, or null
     const float2 *twn;      // [n] twiddles e^{-2 pi i m/N} as [k2][n1]
     int nz, b, ns;
     float sdz;              // sigma * dz
@@ -74,6 +76,8 @@ int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const floa
 // thread-local error message of the C ABI (mset_last_error)
 void set_last_error(const char *msg);
 
+int launch_transmission(const TiltDev *tilts_dev, int ntilts, int n, int nz, int b, int ns, float sdz,
+                        cudaStream_t st);
 int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,
                        const TiltDev *tilts_host, int ntilts, cudaStream_t st);
 

@@ -61,13 +61,46 @@ __device__ __forceinline__ float shift_grid(int k, int n) {
     return (float)i - (float)n * 0.5f;
 }
 
+// Bulk prefetch of `bytes` (multiple of 16) starting at a 16-byte aligned
+// global address into L2, split over the first threads of the CTA
+// (cp.async.bulk.prefetch.L2, no shared memory or registers involved).
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
+    constexpr unsigned kChunk = 16384;
+    const unsigned nchunk = (bytes + kChunk - 1) / kChunk;
+    for (unsigned c = threadIdx.x; c < nchunk; c += blockDim.x) {
+        const unsigned off = c * kChunk;
+        const unsigned len = min(kChunk, bytes - off);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char *)p + off), "r"(len)
+                     : "memory");
+    }
+}
+
+template <class G>
+struct TPre {
+    float2 t[G::R2];  // transmission of the task's elements
+};
+template <class G>
+struct TSPre {
+    float2 t[G::R2];  // transmission
+    float2 w[G::R2];  // saved wave
+};
+
+// shared-memory layout of the position kernel (float2 units after the field)
+template <class G>
+struct Smem {
+    static constexpr int TW = G::N * G::S, E1 = TW + G::N, E2 = E1 + G::N, PY = E2 + G::N, PX = PY + G::N,
+                         END = PX + G::N;
+};
+
 template <class G, int METHOD, int ADJ, int MODE>
 struct PositionKernel {
-    static constexpr int N = G::N, NN = G::N * G::N;
+    static constexpr int N = G::N, NN = G::N * G::N, R1 = G::R1, R2 = G::R2;
 
     // transmission of slab s at (y, x): exp(i sdz sum_{z in slab} V)
-    // (mset.cu:134-153 / STEP02_FORWARD_4D.m:12-20; SSET: all z, mset.cu:391-404)
-    static __device__ __forceinline__ float2 trans(const LaunchArgs &a, const float *V, int s, int y, int x) {
+    // (mset.cu:134-153 / STEP02_FORWARD_4D.m:12-20; SSET: all z, mset.cu:391-404),
+    // read from the precomputed slabs when the tilt has them
+    static __device__ __forceinline__ float2 trans(const LaunchArgs &a, const TiltDev &t, int s, int y, int x) {
+        if (t.T) return t.T[(size_t)s * NN + (size_t)y * N + x];
         int z0, z1;
         if constexpr (METHOD == kSSET) {
             z0 = 0;
@@ -76,7 +109,7 @@ struct PositionKernel {
             z0 = s * a.b;
             z1 = min(z0 + a.b, a.nz);
         }
-        const float *p = V + (size_t)y * N + x;
+        const float *p = t.V + (size_t)y * N + x;
         float acc = 0.f;
         for (int z = z0; z < z1; ++z) acc += p[(size_t)z * NN];
         float sn, cs;
@@ -98,8 +131,21 @@ struct PositionKernel {
         }
     }
 
-    static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, const float2 *tw,
-                               float2 *e1, float2 *e2, double *red, float2 *save) {
+    // propagator / N^2 at scrambled (Ly, Lx): separable product from shared
+    // memory, or the full table in global memory
+    static __device__ __forceinline__ float2 prop(const LaunchArgs &a, const float2 *py, const float2 *px, int Ly,
+                                                  int Lx) {
+        if (a.psep) return cmul(py[Ly], px[Lx]);
+        return __ldg(a.pscr + (size_t)Ly * N + Lx);
+    }
+
+    static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, float2 *save,
+                               double *red) {
+        const float2 *tw = buf + Smem<G>::TW;
+        float2 *e1 = buf + Smem<G>::E1;
+        float2 *e2 = buf + Smem<G>::E2;
+        const float2 *py = buf + Smem<G>::PY;
+        const float2 *px = buf + Smem<G>::PX;
         const int ns = METHOD == kSSET ? 1 : a.ns;
         float *V = t.V;
         const float sxp = t.sx[p], syp = t.sy[p];
@@ -113,81 +159,88 @@ struct PositionKernel {
             sincosf(2.0f * MSET_REF_PI * (s2 * nf / (float)N), &sn, &cs);
             e2[L] = make_float2(cs, sn);
         }
-        __syncthreads();
+        sync_all();
+
+        // prefetch of the transmission of slab s for a row-pass task
+        auto pf_t = [&](int s) {
+            return [&, s](int y, int n1, TPre<G> &pre) {
+#pragma unroll
+                for (int j = 0; j < R2; ++j) pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
+            };
+        };
 
         // ---- incident wave psi0 = F(Q . fs)  (mset.cu:110-131) ----
         col_passB<G, 0, -1>(buf, [&](int y0, int x, float2 *v) {
             const float2 *q = t.Q + (size_t)y0 * N + x;
             const float2 ex = e2[x];
 #pragma unroll
-            for (int j = 0; j < G::R1; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
+            for (int j = 0; j < R1; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
         });
-        __syncthreads();
+        sync_cols<G>();
         col_passA<G, -1, false>(buf, tw);
-        __syncthreads();
+        sync_all();
         row_passB<G, -1>(buf);
-        __syncthreads();
-        if constexpr (MODE == kSim || MODE == kErr) {
-            row_passA<G, -1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
-#pragma unroll
-                for (int j = 0; j < G::R2; ++j) v[j] = cmul(v[j], trans(a, V, 0, y, n1 + G::R1 * j));
-            });
-        } else {
-            row_passA<G, -1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
+        sync_rows();
+        row_passA_pf<G, -1, -1, TPre<G>>(buf, tw, pf_t(0), [&](int y, int n1, float2 *v, const TPre<G> &pre) {
+            if constexpr (MODE != kSim && MODE != kErr) {
                 float2 *sv = save + (size_t)y * N + n1;
 #pragma unroll
-                for (int j = 0; j < G::R2; ++j) {
-                    sv[G::R1 * j] = v[j];
-                    v[j] = cmul(v[j], trans(a, V, 0, y, n1 + G::R1 * j));
-                }
-            });
-        }
-        __syncthreads();
+                for (int j = 0; j < R2; ++j) sv[R1 * j] = v[j];
+            }
+#pragma unroll
+            for (int j = 0; j < R2; ++j) v[j] = cmul(v[j], pre.t[j]);
+        });
+        sync_rows();
 
         // ---- forward slabs (mset.cu:157-183) ----
         if constexpr (METHOD == kMSET) {
             for (int s = 0; s < ns; ++s) {
                 row_passB<G, -1>(buf);
-                __syncthreads();
+                sync_all();
                 col_passA<G, -1, true>(buf, tw);
-                __syncthreads();
+                sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-                    const float2 *pp = a.pscr + (size_t)y0 * N + x;
 #pragma unroll
-                    for (int j = 0; j < G::R1; ++j) v[j] = cmul(v[j], __ldg(pp + (size_t)j * N));
+                    for (int j = 0; j < R1; ++j) v[j] = cmul(v[j], prop(a, py, px, y0 + j, x));
                 });
-                __syncthreads();
+                sync_cols<G>();
                 col_passA<G, +1, false>(buf, tw);
-                __syncthreads();
+                sync_all();
                 row_passB<G, +1>(buf);
-                __syncthreads();
+                sync_rows();
                 const bool last = s + 1 == ns;
-                row_passA<G, +1, -1>(buf, tw, [&](int y, int n1, float2 *v) {
-                    if constexpr (MODE != kSim && MODE != kErr) {
-                        float2 *sv = save + (size_t)(s + 1) * NN + (size_t)y * N + n1;
+                const int sn = last ? s : s + 1;
+                row_passA_pf<G, +1, -1, TPre<G>>(
+                    buf, tw,
+                    [&](int y, int n1, TPre<G> &pre) {
+                        if (!last) pf_t(sn)(y, n1, pre);
+                    },
+                    [&](int y, int n1, float2 *v, const TPre<G> &pre) {
+                        if constexpr (MODE != kSim && MODE != kErr) {
+                            float2 *sv = save + (size_t)(s + 1) * NN + (size_t)y * N + n1;
 #pragma unroll
-                        for (int j = 0; j < G::R2; ++j) sv[G::R1 * j] = v[j];
-                    }
-                    if (!last) {
+                            for (int j = 0; j < R2; ++j) sv[R1 * j] = v[j];
+                        }
+                        if (!last) {
 #pragma unroll
-                        for (int j = 0; j < G::R2; ++j) v[j] = cmul(v[j], trans(a, V, s + 1, y, n1 + G::R1 * j));
-                    }
-                });
-                __syncthreads();
+                            for (int j = 0; j < R2; ++j) v[j] = cmul(v[j], pre.t[j]);
+                        }
+                    });
+                sync_rows();
             }
         }
 
         // ---- far field, error, residual (mset.cu:186-227) ----
         row_passB<G, -1>(buf);
-        __syncthreads();
+        sync_all();
         col_passA<G, -1, true>(buf, tw);
-        __syncthreads();
+        sync_cols<G>();
         double err = 0.0;
         const float *amp = t.amp + (size_t)p * NN;
         if constexpr (MODE == kSim || MODE == kErr) {
             col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-                for (int j = 0; j < G::R1; ++j) {
+                for (int j = 0; j < R1; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     if constexpr (MODE == kSim) {
                         // centred (MATLAB) layout: row r with (r + ceil(N/2)) mod N = ky
@@ -209,13 +262,12 @@ struct PositionKernel {
                 block_sum2<G::NT>(err, dummy, red);
                 if (threadIdx.x == 0) atomicAdd(t.err, err);
             }
-            __syncthreads();
+            sync_all();
             return;
         } else {
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-                const float2 *pp = a.pscr + (size_t)y0 * N + x;
 #pragma unroll
-                for (int j = 0; j < G::R1; ++j) {
+                for (int j = 0; j < R1; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     const float A = sqrtf(a2 + 1e-30f);
                     const float M = meas_amp(amp, y0 + j, x);
@@ -223,33 +275,41 @@ struct PositionKernel {
                     err += (double)(d * d);
                     float2 r = cscale(v[j], 1.0f - M / A);
                     if constexpr (METHOD == kMSET) {
-                        r = cmulc(r, __ldg(pp + (size_t)j * N));  // r * conj(P) / N^2
+                        r = cmulc(r, prop(a, py, px, y0 + j, x));  // r * conj(P) / N^2
                     } else {
                         r = cscale(r, 1.0f / (float)NN);
                     }
                     v[j] = r;
                 }
             });
-            __syncthreads();
+            sync_cols<G>();
         }
 
         // ---- adjoint (mset.cu:232-271; STEP03_BACK.m:12-26) ----
         for (int s = ns - 1; s >= 0; --s) {
+            // REF: the wave saved after slab s (mset.cu:248-251); EXACT: the wave entering slab s
+            const int ws = (METHOD == kSSET || ADJ == kEXACT) ? s : s + 1;
+            // the saved wave was written long ago (DRAM); have it in L2 by the row pass
+            prefetch_l2(save + (size_t)ws * NN, (unsigned)(sizeof(float2) * NN));
             col_passA<G, +1, false>(buf, tw);
-            __syncthreads();
+            sync_all();
             row_passB<G, +1>(buf);
-            __syncthreads();
-            auto gradop = [&](int y, int n1, float2 *v) {
-                // REF: the wave saved after slab s (mset.cu:248-251); EXACT: the wave entering slab s
-                const int ws = (METHOD == kSSET || ADJ == kEXACT) ? s : s + 1;
+            sync_rows();
+            auto pf = [&](int y, int n1, TSPre<G> &pre) {
                 const float2 *sv = save + (size_t)ws * NN + (size_t)y * N + n1;
 #pragma unroll
-                for (int j = 0; j < G::R2; ++j) {
-                    const int x = n1 + G::R1 * j;
-                    const float2 T = trans(a, V, s, y, x);
-                    const float2 psi = sv[G::R1 * j];
+                for (int j = 0; j < R2; ++j) {
+                    pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
+                    pre.w[j] = sv[R1 * j];
+                }
+            };
+            auto gradop = [&](int y, int n1, float2 *v, const TSPre<G> &pre) {
+#pragma unroll
+                for (int j = 0; j < R2; ++j) {
+                    const int x = n1 + R1 * j;
+                    const float2 T = pre.t[j];
                     // g = i conj(T) conj(psi) chi
-                    const float2 u = cmulc(cmulc(v[j], T), psi);
+                    const float2 u = cmulc(cmulc(v[j], T), pre.w[j]);
                     const float gre = -u.y;  // Re(i u)
                     if constexpr (MODE == kSeq) {
                         int z0, z1;
@@ -270,21 +330,20 @@ struct PositionKernel {
                 }
             };
             if (s > 0) {
-                row_passA<G, +1, -1>(buf, tw, gradop);
-                __syncthreads();
+                row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop);
+                sync_rows();
                 row_passB<G, -1>(buf);
-                __syncthreads();
+                sync_all();
                 col_passA<G, -1, true>(buf, tw);
-                __syncthreads();
+                sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-                    const float2 *pp = a.pscr + (size_t)y0 * N + x;
 #pragma unroll
-                    for (int j = 0; j < G::R1; ++j) v[j] = cmulc(v[j], __ldg(pp + (size_t)j * N));
+                    for (int j = 0; j < R1; ++j) v[j] = cmulc(v[j], prop(a, py, px, y0 + j, x));
                 });
-                __syncthreads();
+                sync_cols<G>();
             } else {
-                row_passA<G, +1, 0>(buf, tw, gradop);
-                __syncthreads();
+                row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop);
+                sync_all();
             }
         }
         // buf now holds chi0 (real space, natural order); save[0] holds psi0.
@@ -309,22 +368,22 @@ struct PositionKernel {
                 pdy += (double)(dy.x * c0.x + dy.y * c0.y);
             }
         }
-        __syncthreads();
+        sync_all();
 
         // ---- probe direction: d = F^{-1}(chi0) fs(-s), accumulated in the
         //      F^{-1}(probe) domain (mset.cu:288-312) ----
         row_passA<G, 0, +1>(buf, tw, NoOp{});
-        __syncthreads();
+        sync_rows();
         row_passB<G, +1>(buf);
-        __syncthreads();
+        sync_all();
         col_passA<G, +1, true>(buf, tw);
-        __syncthreads();
+        sync_cols<G>();
         const float inv = 1.0f / (float)NN;
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
             const float2 ex = e2[x];
             const float kx = 2.0f * MSET_REF_PI * shift_grid(G::scr(x), N) / (float)N;
 #pragma unroll
-            for (int j = 0; j < G::R1; ++j) {
+            for (int j = 0; j < R1; ++j) {
                 const size_t li = (size_t)(y0 + j) * N + x;
                 const float2 fs = cmul(e1[y0 + j], ex);
                 const float2 d = cscale(cmulc(v[j], fs), inv);
@@ -362,32 +421,38 @@ struct PositionKernel {
                 t.posdir[2 * p + 1] = pdy;
             }
         }
-        __syncthreads();
+        sync_all();
     }
 };
 
 template <class G>
-__device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *twn) {
-    for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
+__device__ __forceinline__ void load_tables(float2 *buf, const LaunchArgs &a) {
+    float2 *tw = buf + Smem<G>::TW;
+    float2 *py = buf + Smem<G>::PY;
+    float2 *px = buf + Smem<G>::PX;
+    for (int i = threadIdx.x; i < G::N; i += G::NT) {
+        tw[i] = a.twn[i];
+        if (a.psep) {
+            py[i] = a.psep[i];
+            px[i] = a.psep[G::N + i];
+        }
+    }
 }
 
 template <class G, int METHOD, int ADJ, int MODE>
 __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a) {
     extern __shared__ __align__(16) float2 smem[];
     float2 *buf = smem;
-    float2 *tw = buf + G::N * G::S;
-    float2 *e1 = tw + G::N;
-    float2 *e2 = e1 + G::N;
-    double *red = reinterpret_cast<double *>(e2 + G::N);
+    double *red = reinterpret_cast<double *>(buf + Smem<G>::END);
     __shared__ int s_item;
-    load_twiddles<G>(tw, a.twn);
+    load_tables<G>(buf, a);
     const int nsave = (METHOD == kSSET ? 1 : a.ns) + 1;
     float2 *save = a.save + (size_t)blockIdx.x * nsave * G::N * G::N;
     __syncthreads();
     using K = PositionKernel<G, METHOD, ADJ, MODE>;
     if constexpr (MODE == kSeq) {
         const TiltDev &t = a.tilts[a.seq_tilt];
-        for (int p = 0; p < t.npos; ++p) K::run(a, t, p, buf, tw, e1, e2, red, save);
+        for (int p = 0; p < t.npos; ++p) K::run(a, t, p, buf, save, red);
     } else {
         for (;;) {
             if (threadIdx.x == 0) s_item = (int)atomicAdd(a.counter, 1u);
@@ -396,7 +461,7 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
             __syncthreads();
             if (it >= a.nitems) break;
             const int2 tp = a.items[it];
-            K::run(a, a.tilts[tp.x], tp.y, buf, tw, e1, e2, red, save);
+            K::run(a, a.tilts[tp.x], tp.y, buf, save, red);
         }
     }
 }
@@ -440,7 +505,7 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
     extern __shared__ __align__(16) float2 smem[];
     float2 *buf = smem;
     float2 *tw = buf + G::N * G::S;
-    load_twiddles<G>(tw, twn);
+    for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
     __syncthreads();
     constexpr int N = G::N;
     if constexpr (TO_Q) {
@@ -477,7 +542,7 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
 
 template <class G>
 inline size_t smem_bytes() {
-    return sizeof(float2) * ((size_t)G::N * G::S + 3 * G::N) + sizeof(double) * 2 * ((G::NT + 31) / 32);
+    return sizeof(float2) * (size_t)Smem<G>::END + sizeof(double) * 2 * ((G::NT + 31) / 32);
 }
 
 template <class G, int METHOD, int ADJ, int MODE>
