@@ -159,6 +159,29 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 
+/* ---- Fourier-shear tilt rotation --------------------------------------------
+ * Func_rot_3Dvol_FourierShear (inverse = 0) and Func_inv_rot_3Dvol_FourierShear
+ * (inverse = 1) (func_lib/Func_rot_3Dvol_FourierShear.m:5-19,
+ * Func_inv_rot_3Dvol_FourierShear.m:5-20, Func_rotate_3Dvol_ROTmat_FourierShear.m:14-134):
+ * rotation by the quaternion axes vec1..vec3 and angles (phi, theta, psi) in
+ * degrees, split into sub-rotations of at most 11 degrees of four Fourier
+ * shears each.  vol_in / vol_out: host [n][n][n] float (MATLAB n x n x n),
+ * may alias.  All angles within 0.5 degrees: copied unchanged, as the
+ * reference does.  Cubic volumes with n in {24, 32, 48, 64, 96, 128, 160}. */
+int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int n, const float *vec1,
+                       const float *vec2, const float *vec3, double phi, double theta, double psi, int inverse);
+
+/* ---- TV regularisation -------------------------------------------------------
+ * TV_FISTA_method (fista = 1, func_lib/TV_FISTA_method.m:5-38) or TV_method
+ * (fista = 0, func_lib/TV_method.m:5-28) on a 3D volume: niter projected
+ * gradient iterations on the dual field (tau = 1/12, periodic differences),
+ * output = input - lambda div(P), tv_error = lambda * sum |grad(output)|.
+ * vol: host [n3][n2][n1] float, replaced by the output.  Dual variables in
+ * FP32 (the reference's arithmetic is single once it meets the single input),
+ * FISTA momentum step in FP64, error in FP64. */
+int mset_tv(mset_session *s, float *vol, int n1, int n2, int n3, double lambda, int niter, int fista,
+            double *tv_error);
+
 /* ---- allocation-free batched pass -------------------------------------------
  * Has no counterpart in the reference.  For callers that cannot allocate
  * device memory (work issued while a CUDA graph is being captured, device

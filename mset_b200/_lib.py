@@ -50,6 +50,9 @@ SIGNATURES = {
     "mset_batch_get_tilt": (C.c_int, [C.c_void_p, C.c_int, _F, _F, _F, _F]),
     "mset_batch_time": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "mset_batch_launch_count": (C.c_int, [C.c_void_p]),
+    "mset_rotate_volume": (C.c_int, [C.c_void_p, _F, _F, C.c_int, _F, _F, _F, C.c_double, C.c_double, C.c_double,
+                                     C.c_int]),
+    "mset_tv": (C.c_int, [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D]),
     "mset_batch_gradient_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_float, C.c_float, C.c_int] + [C.c_void_p] * 10),
 }

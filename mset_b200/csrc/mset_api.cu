@@ -10,6 +10,8 @@
 
 #include "../../include/mset_b200.h"
 #include "mset_kernels.cuh"
+#include "mset_rotate.cuh"
+#include "mset_volume.cuh"
 
 using namespace mset;
 
@@ -109,6 +111,13 @@ struct mset_session {
     int save_slots = 0;
     std::vector<TiltDev> h_tilts;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // TV work buffers
+    DevBuf<float> tv_in, tv_out, tv_P, tv_Y, tv_D;
+    DevBuf<double> tv_err;
+    // rotation work buffers
+    DevBuf<float> rot_vol;
+    DevBuf<float2> rot_S, rot_tw;
+    int rot_n = 0;
 };
 
 namespace {
@@ -709,6 +718,73 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_pass = ms / reps;
+    return 0;
+}
+
+// ---- Fourier-shear rotation -------------------------------------------------
+static int rot_prepare(mset_session *s, int n) {
+    if (!rot_supported(n))
+        return fail(MSET_E_UNSUPPORTED, "rotation of a %d^3 volume has no compiled kernel "
+                                        "(supported: 24, 32, 48, 64, 96, 128, 160)", n);
+    const size_t n3 = (size_t)n * n * n;
+    CK(s->rot_vol.ensure(n3));
+    CK(s->rot_S.ensure(n3));
+    if (s->rot_n != n) {
+        std::vector<float2> h;
+        rot_twiddles(n, h);
+        CK(s->rot_tw.ensure(n));
+        CK(cudaMemcpyAsync(s->rot_tw.p, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        s->rot_n = n;
+    }
+    return 0;
+}
+
+int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int n, const float *vec1,
+                       const float *vec2, const float *vec3, double phi, double theta, double psi, int inverse) {
+    if (!s || !vol_in || !vol_out || !vec1 || !vec2 || !vec3) return fail(MSET_E_ARG, "null argument");
+    if (n <= 1) return fail(MSET_E_ARG, "bad volume size %d", n);
+    int rc = set_device(s);
+    if (rc) return rc;
+    rc = rot_prepare(s, n);
+    if (rc) return rc;
+    const double v1[3] = {vec1[0], vec1[1], vec1[2]}, v2[3] = {vec2[0], vec2[1], vec2[2]},
+                 v3[3] = {vec3[0], vec3[1], vec3[2]};
+    RotPlan pl;
+    rot_plan(v1, v2, v3, phi, theta, psi, inverse != 0, &pl);
+    const size_t n3 = (size_t)n * n * n;
+    CK(cudaMemcpyAsync(s->rot_vol.p, vol_in, sizeof(float) * n3, cudaMemcpyHostToDevice, s->st));
+    CKL(rot_apply(pl, n, s->rot_vol.p, s->rot_vol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
+    CK(cudaMemcpyAsync(vol_out, s->rot_vol.p, sizeof(float) * n3, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+// ---- TV / TV-FISTA ----------------------------------------------------------
+int mset_tv(mset_session *s, float *vol, int n1, int n2, int n3, double lambda, int niter, int fista,
+            double *tv_error) {
+    if (!s || !vol) return fail(MSET_E_ARG, "null argument");
+    if (n1 <= 0 || n2 <= 0 || n3 <= 0 || niter < 0 || !(lambda > 0))
+        return fail(MSET_E_ARG, "need positive sizes, niter >= 0 and lambda > 0");
+    int rc = set_device(s);
+    if (rc) return rc;
+    const size_t V = (size_t)n1 * n2 * n3;
+    CK(s->tv_in.ensure(V));
+    CK(s->tv_out.ensure(V));
+    CK(s->tv_P.ensure(3 * V));
+    CK(s->tv_Y.ensure(3 * V));
+    CK(s->tv_D.ensure(V));
+    CK(s->tv_err.ensure(1));
+    CK(cudaMemcpyAsync(s->tv_in.p, vol, sizeof(float) * V, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
+    TvArgs a{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, n1, n2, n3, lambda, niter, fista ? 1 : 0,
+             s->tv_err.p};
+    CKL(tv_prox(a, s->st), "tv");
+    CK(cudaMemcpyAsync(vol, s->tv_out.p, sizeof(float) * V, cudaMemcpyDeviceToHost, s->st));
+    double e = 0;
+    CK(cudaMemcpyAsync(&e, s->tv_err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (tv_error) *tv_error = e;
     return 0;
 }
 

@@ -1,0 +1,230 @@
+// mset_volume.cu -- volume kernels of the reconstruction update:
+// TV / TV-FISTA proximal operator (func_lib/TV_method.m:5-28 and helpers
+// :32-83, func_lib/TV_FISTA_method.m:5-38), positivity
+// (Run_MSET_recon.m:183-185), max-normalisation (Run_MSET_recon.m:268-270),
+// and the glue between beam-frame slab gradients and the lab-frame volume.
+//
+// All stencils are periodic (MATLAB circshift).  Volumes are C order
+// [n3][n2][n1] = MATLAB (n1, n2, n3); MATLAB dim 1 is the fastest axis.
+// HBM/L2-bound elementwise work: grid-stride loops over 148 x 8 CTAs.
+#include <cmath>
+
+#include "mset_volume.cuh"
+
+namespace mset {
+
+namespace {
+constexpr int kThreads = 256;
+
+inline int grid_for(long total) {
+    long g = (total + kThreads - 1) / kThreads;
+    return (int)std::min<long>(std::max<long>(g, 1), 148L * 8);
+}
+
+__device__ __forceinline__ long wrap(long i, long n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// D = TV_div(Y) - in / lambda   (the argument of TV_del in TV_method.m:21)
+__global__ void k_tv_d(const float *Y, const float *in, float *D, int n1, int n2, int n3, float inv_lam) {
+    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
+        const long m1 = r - i1 + wrap(i1 - 1, n1);
+        const long m2 = r + (wrap(i2 - 1, n2) - i2) * s2;
+        const long m3 = r + (wrap(i3 - 1, n3) - i3) * s3;
+        const float d = Y[r] + Y[V + r] + Y[2 * V + r] - Y[m1] - Y[V + m2] - Y[2 * V + m3];
+        D[r] = d - in[r] * inv_lam;
+    }
+}
+
+// P <- TV_project(src + tau TV_del(D)); FISTA: Y <- P + m (P - P_old) in FP64
+__global__ void k_tv_step(float *P, float *Y, const float *D, int n1, int n2, int n3, float tau, double m,
+                          int fista) {
+    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
+        const float d0 = D[r];
+        const float t1 = tau * (D[r - i1 + wrap(i1 + 1, n1)] - d0);
+        const float t2 = tau * (D[r + (wrap(i2 + 1, n2) - i2) * s2] - d0);
+        const float t3 = tau * (D[r + (wrap(i3 + 1, n3) - i3) * s3] - d0);
+        const float *src = fista ? Y : P;
+        const float q1 = src[r] + t1, q2 = src[V + r] + t2, q3 = src[2 * V + r] + t3;
+        const float nrm = sqrtf(fmaxf(1.0f, q1 * q1 + q2 * q2 + q3 * q3));
+        const float p1 = q1 / nrm, p2 = q2 / nrm, p3 = q3 / nrm;
+        if (fista) {
+            const double o1 = P[r], o2 = P[V + r], o3 = P[2 * V + r];
+            Y[r] = (float)(p1 + m * (p1 - o1));
+            Y[V + r] = (float)(p2 + m * (p2 - o2));
+            Y[2 * V + r] = (float)(p3 + m * (p3 - o3));
+        }
+        P[r] = p1;
+        P[V + r] = p2;
+        P[2 * V + r] = p3;
+    }
+}
+
+// out = in - lambda TV_div(P)   (TV_method.m:26)
+__global__ void k_tv_out(const float *P, const float *in, float *out, int n1, int n2, int n3, float lam) {
+    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
+        const long m1 = r - i1 + wrap(i1 - 1, n1);
+        const long m2 = r + (wrap(i2 - 1, n2) - i2) * s2;
+        const long m3 = r + (wrap(i3 - 1, n3) - i3) * s3;
+        const float dv = P[r] + P[V + r] + P[2 * V + r] - P[m1] - P[V + m2] - P[2 * V + m3];
+        out[r] = in[r] - lam * dv;
+    }
+}
+
+// err += lambda sum |TV_del(u)|   (TV_method.m:27, 71-83), FP64 accumulation
+__global__ void k_tv_err(const float *u, int n1, int n2, int n3, double lam, double *err) {
+    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
+    double acc = 0.0;
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
+        const float u0 = u[r];
+        const float d1 = u[r - i1 + wrap(i1 + 1, n1)] - u0;
+        const float d2 = u[r + (wrap(i2 + 1, n2) - i2) * s2] - u0;
+        const float d3 = u[r + (wrap(i3 + 1, n3) - i3) * s3] - u0;
+        acc += sqrt((double)d1 * d1 + (double)d2 * d2 + (double)d3 * d3);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(err, lam * acc);
+}
+
+// in = vol / max(vol) with max from *mx; the max itself by k_max
+__global__ void k_max(const float *v, long n, unsigned *mx_bits) {
+    float m = -INFINITY;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        m = fmaxf(m, v[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // order-preserving integer image of the float
+    if ((threadIdx.x & 31) == 0) {
+        unsigned b = __float_as_uint(m);
+        b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+        atomicMax(mx_bits, b);
+    }
+}
+
+__global__ void k_bits_to_float(const unsigned *mx_bits, float *mx) {
+    unsigned b = *mx_bits;
+    b = (b & 0x80000000u) ? (b & 0x7fffffffu) : ~b;
+    *mx = __uint_as_float(b);
+}
+
+__global__ void k_scale(const float *v, float *out, long n, const float *div) {
+    const float d = *div;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = v[i] / d;
+}
+
+__global__ void k_mul(const float *v, float *out, long n, const float *mul) {
+    const float m = *mul;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = v[i] * m;
+}
+
+__global__ void k_positivity(float *v, long n) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        if (v[i] < 0.f) v[i] = 0.f;
+}
+
+// beam-frame volume of a tilt: V[z][y][x] (n x n window) = centred copy of
+// the rotated nv^3 volume (zero elsewhere): the volume zero-padded laterally
+// to the probe window (exact under the periodic multislice: V = 0 gives T = 1)
+__global__ void k_pad(const float *src, float *V, int nv, int n) {
+    const long nn = (long)n * n, total = nn * nv;
+    const int o = (n - nv) / 2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(i / nn), y = (int)((i / n) % n), x = (int)(i % n);
+        const int yy = y - o, xx = x - o;
+        V[i] = (yy >= 0 && yy < nv && xx >= 0 && xx < nv) ? src[((long)z * nv + yy) * nv + xx] : 0.f;
+    }
+}
+
+// lab-frame gradient contribution of a tilt: slab gradient G[s] (n x n,
+// FP64) replicated over the slab's voxels and cropped to the nv^3 volume
+__global__ void k_slab_to_volume(const double *G, float *out, int nv, int n, int b) {
+    const long total = (long)nv * nv * nv;
+    const int o = (n - nv) / 2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(i / ((long)nv * nv)), y = (int)((i / nv) % nv), x = (int)(i % nv);
+        out[i] = (float)G[(long)(z / b) * n * n + (long)(y + o) * n + (x + o)];
+    }
+}
+
+__global__ void k_accumulate(const float *g, double *acc, long n, int zero) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        acc[i] = (zero ? 0.0 : acc[i]) + (double)g[i];
+}
+
+// rec += step0 * acc
+__global__ void k_update(float *rec, const double *acc, long n, float step0) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        rec[i] += step0 * (float)acc[i];
+}
+}  // namespace
+
+int tv_prox(const TvArgs &a, cudaStream_t st) {
+    const long V = (long)a.n1 * a.n2 * a.n3;
+    const int g = grid_for(V);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(a.P, 0, sizeof(float) * 3 * V, st)) != cudaSuccess) return (int)e;
+    if ((e = cudaMemsetAsync(a.Y, 0, sizeof(float) * 3 * V, st)) != cudaSuccess) return (int)e;
+    const float tau = 1.0f / 12.0f;  // 3D (TV_method.m:13-16)
+    double t = 1.0;
+    for (int it = 0; it < a.niter; ++it) {
+        const double t0 = t;
+        t = (1.0 + std::sqrt(1.0 + 4.0 * t0 * t0)) / 2.0;  // TV_FISTA_method.m:31
+        const double m = (t0 - 1.0) / t;
+        k_tv_d<<<g, kThreads, 0, st>>>(a.fista ? a.Y : a.P, a.in, a.D, a.n1, a.n2, a.n3, (float)(1.0 / a.lambda));
+        k_tv_step<<<g, kThreads, 0, st>>>(a.P, a.Y, a.D, a.n1, a.n2, a.n3, tau, m, a.fista);
+    }
+    k_tv_out<<<g, kThreads, 0, st>>>(a.P, a.in, a.out, a.n1, a.n2, a.n3, (float)a.lambda);
+    if (a.err) k_tv_err<<<g, kThreads, 0, st>>>(a.out, a.n1, a.n2, a.n3, a.lambda, a.err);
+    return (int)cudaGetLastError();
+}
+
+int vol_max(const float *v, long n, unsigned *bits, float *mx, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(bits, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return (int)e;
+    k_max<<<grid_for(n), kThreads, 0, st>>>(v, n, bits);
+    k_bits_to_float<<<1, 1, 0, st>>>(bits, mx);
+    return (int)cudaGetLastError();
+}
+
+int vol_scale(const float *v, float *out, long n, const float *div, cudaStream_t st) {
+    k_scale<<<grid_for(n), kThreads, 0, st>>>(v, out, n, div);
+    return (int)cudaGetLastError();
+}
+
+int vol_mul(const float *v, float *out, long n, const float *mul, cudaStream_t st) {
+    k_mul<<<grid_for(n), kThreads, 0, st>>>(v, out, n, mul);
+    return (int)cudaGetLastError();
+}
+
+int vol_positivity(float *v, long n, cudaStream_t st) {
+    k_positivity<<<grid_for(n), kThreads, 0, st>>>(v, n);
+    return (int)cudaGetLastError();
+}
+
+int vol_pad(const float *src, float *V, int nv, int n, cudaStream_t st) {
+    k_pad<<<grid_for((long)n * n * nv), kThreads, 0, st>>>(src, V, nv, n);
+    return (int)cudaGetLastError();
+}
+
+int vol_slab_to_volume(const double *G, float *out, int nv, int n, int b, cudaStream_t st) {
+    k_slab_to_volume<<<grid_for((long)nv * nv * nv), kThreads, 0, st>>>(G, out, nv, n, b);
+    return (int)cudaGetLastError();
+}
+
+int vol_accumulate(const float *g, double *acc, long n, bool zero, cudaStream_t st) {
+    k_accumulate<<<grid_for(n), kThreads, 0, st>>>(g, acc, n, zero ? 1 : 0);
+    return (int)cudaGetLastError();
+}
+
+int vol_update(float *rec, const double *acc, long n, float step0, cudaStream_t st) {
+    k_update<<<grid_for(n), kThreads, 0, st>>>(rec, acc, n, step0);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace mset

@@ -167,7 +167,9 @@ def make_specimen(cfg: Config, with_volumes: bool = True) -> Specimen:
     vols = []
     if with_volumes:
         for th in angles[:, 1]:
-            R = rot_y(th)
+            # beam frame of tilt th: the reference's Func_inv_rot_3Dvol_FourierShear
+            # with (phi, theta, psi) = (0, th, 0) maps (x, 0, 0) to (x cos th, 0, x sin th)
+            R = rot_y(-th)
             v = voxelise(pos @ R.T, peak, cfg.vol, cfg.dx, cfg.blob_sigma)
             vols.append(pad_lateral(v, cfg.window).astype(np.float32))
     n = cfg.window

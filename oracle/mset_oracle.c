@@ -594,3 +594,283 @@ int orc_max_threads(void) {
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------- */
+/* Fourier-shear 3D rotation (Welling et al. 2006) as in the reference:      */
+/*   func_lib/Func_rot_3Dvol_FourierShear.m:5-19,                            */
+/*   Func_inv_rot_3Dvol_FourierShear.m:5-20, MatrixQuaternionRot.m:1-11,     */
+/*   Func_rotate_3Dvol_ROTmat_FourierShear.m:14-134,                         */
+/*   My_obtain_quaternion_from_matrix.m:11-39,                               */
+/*   calculate_S_matrices_for3DFourierShearRot_perm_ver1.m:16-93,            */
+/*   ..._backward_ver1.m:16-91, SheerTransforms_for3Drot.m:16-49.            */
+/* Volume layout: C [n3][n2][n1] = MATLAB (n1, n2, n3).                      */
+/* ------------------------------------------------------------------------- */
+static void quat_rot(const double *v, double theta_deg, double R[3][3]) {
+    double th = theta_deg * M_PI / 180.0;
+    double nv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double w = cos(th / 2), x = -sin(th / 2) * v[0] / nv, y = -sin(th / 2) * v[1] / nv, z = -sin(th / 2) * v[2] / nv;
+    R[0][0] = 1 - 2 * y * y - 2 * z * z; R[0][1] = 2 * x * y + 2 * w * z; R[0][2] = 2 * x * z - 2 * w * y;
+    R[1][0] = 2 * x * y - 2 * w * z; R[1][1] = 1 - 2 * x * x - 2 * z * z; R[1][2] = 2 * y * z + 2 * w * x;
+    R[2][0] = 2 * x * z + 2 * w * y; R[2][1] = 2 * y * z - 2 * w * x; R[2][2] = 1 - 2 * x * x - 2 * y * y;
+}
+
+static void matmul3(double A[3][3], double B[3][3], double C[3][3]) {
+    double T[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T[i][j] = 0;
+            for (int k = 0; k < 3; ++k) T[i][j] += A[i][k] * B[k][j];
+        }
+    memcpy(C, T, sizeof T);
+}
+
+static void inv3(double A[3][3], double B[3][3]) {
+    double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                 A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    double T[3][3];
+    T[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+    T[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+    T[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+    T[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+    T[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+    T[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) / det;
+    T[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+    T[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+    T[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
+    memcpy(B, T, sizeof T);
+}
+
+static void quat_from_matrix(double M[3][3], double *qx, double *qy, double *qz, double *qw) {
+    double Tr = M[0][0] + M[1][1] + M[2][2], S;
+    if (Tr > 0) {
+        S = sqrt(Tr + 1) * 2;
+        *qw = 0.25 * S; *qx = (M[2][1] - M[1][2]) / S; *qy = (M[0][2] - M[2][0]) / S; *qz = (M[1][0] - M[0][1]) / S;
+    } else if (M[0][0] > M[1][1] && M[0][0] > M[2][2]) {
+        S = sqrt(1.0 + M[0][0] - M[1][1] - M[2][2]) * 2;
+        *qw = (M[2][1] - M[1][2]) / S; *qx = 0.25 * S; *qy = (M[0][1] + M[1][0]) / S; *qz = (M[0][2] + M[2][0]) / S;
+    } else if (M[1][1] > M[2][2]) {
+        S = sqrt(1.0 + M[1][1] - M[0][0] - M[2][2]) * 2;
+        *qw = (M[0][2] - M[2][0]) / S; *qx = (M[0][1] + M[1][0]) / S; *qy = 0.25 * S; *qz = (M[1][2] + M[2][1]) / S;
+    } else {
+        S = sqrt(1.0 + M[2][2] - M[0][0] - M[1][1]) * 2;
+        *qw = (M[1][0] - M[0][1]) / S; *qx = (M[0][2] + M[2][0]) / S; *qy = (M[1][2] + M[2][1]) / S; *qz = 0.25 * S;
+    }
+}
+
+/* shear coefficients a..h for one permutation; returns absSum (INF if singular) */
+static double shear_coeffs(double X0, double Y0, double Z0, double W, int perm, int backward, double co[8]) {
+    double in[3] = {X0, Y0, Z0};
+    /* circshift([X,Y,Z], [0 -perm]): element i takes in[(i + perm) mod 3] */
+    double X = in[(0 + perm) % 3], Y = in[(1 + perm) % 3], Z = in[(2 + perm) % 3];
+    if (backward) W = -W;
+    double a, b, c, d, e, f, g, h;
+    if (fabs(Y * Z - X * W) > 1e-5 && fabs(X * Y - Z * W) > 1e-5) {
+        a = (X * X + Y * Y) / (Y * Z - X * W);
+        b = (Y * Y - Z * Z) / (X * Y - Z * W) - 2 * (Y * Z * (X * X + Y * Y)) / (X * Y - Z * W) / (Y * Z - X * W);
+        c = 2 * Y * Z / (X * Y - Z * W);
+        d = 2 * (X * W - Y * Z);
+        e = 2 * (X * Y - Z * W);
+        f = -2 * X * Y / (Y * Z - X * W);
+        g = (X * X - Y * Y) / (Y * Z - X * W) + 2 * X * Y * (Y * Y + Z * Z) / (X * Y - Z * W) / (Y * Z - X * W);
+        h = (-1 + X * X + W * W) / (X * Y - Z * W);
+    } else if (fabs(Y) < 1e-6) {
+        a = -X / W; b = Z / W; c = 0; d = 2 * X * W; e = -2 * Z * W; f = 0; g = -X / W; h = Z / W;
+    } else {
+        return INFINITY;
+    }
+    double v[8] = {a, b, c, d, e, f, g, h};
+    double s = 0;
+    for (int i = 0; i < 8; ++i) {
+        co[i] = backward ? -v[i] : v[i];
+        s += fabs(v[i]);
+    }
+    return s;
+}
+
+/* grid value after ifftshift(k - round((n+1)/2)) with the Nyquist index zeroed
+ * (Func_rotate_3Dvol_ROTmat_FourierShear.m:70-90); *nyq = 1 at that index */
+static double rot_grid(int i, int n, int *nyq) {
+    int h = (n + 1) / 2;          /* ceil(n/2) */
+    int k = (i - h) % n; if (k < 0) k += n;  /* ifftshift: out[i] = v[(i - ceil(n/2)) mod n] */
+    double c = floor((n + 1) / 2.0 + 0.5);
+    double val = (double)(k + 1) - c;
+    *nyq = (n % 2 == 0) && (i == (int)c - 1);
+    return *nyq ? 0.0 : val;
+}
+
+typedef struct { int n[3]; fftplan pl[3]; cd *buf1, *buf2; } rotctx;
+
+/* one shear along MATLAB dimension dim (1, 2, 3) with coefficients (ca, cb) */
+static void shear(rotctx *r, cd *V, int dim, double ca, double cb) {
+    int n1 = r->n[0], n2 = r->n[1], n3 = r->n[2];
+    long s1 = 1, s2 = n1, s3 = (long)n1 * n2;
+    int other[2];
+    if (dim == 1) { other[0] = 3; other[1] = 2; }
+    else if (dim == 2) { other[0] = 3; other[1] = 1; }
+    else { other[0] = 2; other[1] = 1; }
+    long st[4] = {0, s1, s2, s3};
+    int nn[4] = {0, n1, n2, n3};
+    /* forward FFTs along the two other dims */
+    for (int o = 0; o < 2; ++o) {
+        int d = other[o];
+        /* loop over all lines along d */
+        for (long base = 0; base < (long)n1 * n2 * n3; ++base) {
+            int i1 = base % n1, i2 = (base / n1) % n2, i3 = base / ((long)n1 * n2);
+            int idx[4] = {0, i1, i2, i3};
+            if (idx[d] != 0) continue;
+            fft1(&r->pl[d - 1], V + base, st[d], -1, r->buf1, r->buf2);
+        }
+    }
+    for (int i3 = 0; i3 < n3; ++i3)
+        for (int i2 = 0; i2 < n2; ++i2)
+            for (int i1 = 0; i1 < n1; ++i1) {
+                int q1, q2, q3;
+                double g1 = rot_grid(i1, n1, &q1), g2 = rot_grid(i2, n2, &q2), g3 = rot_grid(i3, n3, &q3);
+                if (q1 || q2 || q3) continue; /* nx = ny = nz = 0 on any Nyquist plane: phase 0 */
+                double ph;
+                if (dim == 1) ph = 2 * M_PI * ((double)n2 / n1 * ca * g2 / n2 + (double)n3 / n1 * cb * g3 / n3) * g1;
+                else if (dim == 2) ph = 2 * M_PI * ((double)n1 / n2 * cb * g1 / n1 + (double)n3 / n2 * ca * g3 / n3) * g2;
+                else ph = 2 * M_PI * ((double)n1 / n3 * ca * g1 / n1 + (double)n2 / n3 * cb * g2 / n2) * g3;
+                V[(long)i3 * s3 + (long)i2 * s2 + i1] *= cos(ph) + I * sin(ph);
+            }
+    for (int o = 0; o < 2; ++o) {
+        int d = other[o];
+        double sc = 1.0 / nn[d];
+        for (long base = 0; base < (long)n1 * n2 * n3; ++base) {
+            int i1 = base % n1, i2 = (base / n1) % n2, i3 = base / ((long)n1 * n2);
+            int idx[4] = {0, i1, i2, i3};
+            if (idx[d] != 0) continue;
+            fft1(&r->pl[d - 1], V + base, st[d], +1, r->buf1, r->buf2);
+            for (int k = 0; k < nn[d]; ++k) V[base + k * st[d]] *= sc;
+        }
+    }
+}
+
+/* Func_rotate_3Dvol_ROTmat_FourierShear(vol, MAT, rotStepInit), MAT row-major */
+static void rotate_rotmat(double *vol, int n1, int n2, int n3, double M[3][3], double rotStepInit) {
+    double qx, qy, qz, qw;
+    quat_from_matrix(M, &qx, &qy, &qz, &qw);
+    double Ang = acos(qw) * 180.0 / M_PI * 2;
+    double nv = sqrt(qx * qx + qy * qy + qz * qz);
+    double Vec[3] = {qx / nv, qy / nv, qz / nv};
+    int numStep = (int)floor(Ang / rotStepInit) + 1;
+    double rotStep = Ang / numStep;
+    double w = cos(rotStep / 2 * M_PI / 180), x = -sin(rotStep / 2 * M_PI / 180) * Vec[0],
+           y = -sin(rotStep / 2 * M_PI / 180) * Vec[1], z = -sin(rotStep / 2 * M_PI / 180) * Vec[2];
+    double cf[3][8], cb[3][8], sf[3], sb[3];
+    for (int i = 1; i <= 3; ++i) {
+        sf[i - 1] = shear_coeffs(x, y, z, w, i, 0, cf[i - 1]);
+        sb[i - 1] = shear_coeffs(x, y, z, w, i, 1, cb[i - 1]);
+    }
+    int mf = 0, mb = 0;
+    for (int i = 1; i < 3; ++i) {
+        if (sf[i] < sf[mf]) mf = i;
+        if (sb[i] < sb[mb]) mb = i;
+    }
+    int fwd = sf[mf] < sb[mb];
+    int mI = (fwd ? mf : mb) + 1; /* MATLAB 1-based index */
+    double *co = fwd ? cf[mf] : cb[mb];
+    rotctx r;
+    r.n[0] = n1; r.n[1] = n2; r.n[2] = n3;
+    int mx = n1 > n2 ? n1 : n2; if (n3 > mx) mx = n3;
+    for (int d = 0; d < 3; ++d) plan_init(&r.pl[d], r.n[d]);
+    r.buf1 = malloc(sizeof(cd) * mx);
+    r.buf2 = malloc(sizeof(cd) * mx);
+    long nv3 = (long)n1 * n2 * n3;
+    cd *S = malloc(sizeof(cd) * nv3);
+    /* SheerVol = ifftshift(initVol) */
+    int h1 = (n1 + 1) / 2, h2 = (n2 + 1) / 2, h3 = (n3 + 1) / 2;
+    for (int i3 = 0; i3 < n3; ++i3)
+        for (int i2 = 0; i2 < n2; ++i2)
+            for (int i1 = 0; i1 < n1; ++i1)
+                S[(long)((i3 + h3) % n3) * n1 * n2 + (long)((i2 + h2) % n2) * n1 + (i1 + h1) % n1] =
+                    vol[(long)i3 * n1 * n2 + (long)i2 * n1 + i1];
+    for (int st = 0; st < numStep; ++st) {
+        if (fwd) {
+            shear(&r, S, (mI + 1) % 3 + 1, co[6], co[7]);
+            shear(&r, S, mI % 3 + 1, co[4], co[5]);
+            shear(&r, S, (mI + 2) % 3 + 1, co[2], co[3]);
+            shear(&r, S, (mI + 1) % 3 + 1, co[0], co[1]);
+        } else {
+            shear(&r, S, (mI + 1) % 3 + 1, co[0], co[1]);
+            shear(&r, S, (mI + 2) % 3 + 1, co[2], co[3]);
+            shear(&r, S, mI % 3 + 1, co[4], co[5]);
+            shear(&r, S, (mI + 1) % 3 + 1, co[6], co[7]);
+        }
+        for (long i = 0; i < nv3; ++i) S[i] = creal(S[i]);
+    }
+    /* RotVol = fftshift(SheerVol): out[(i + floor(n/2)) mod n] = S[i] */
+    for (int i3 = 0; i3 < n3; ++i3)
+        for (int i2 = 0; i2 < n2; ++i2)
+            for (int i1 = 0; i1 < n1; ++i1)
+                vol[(long)((i3 + n3 / 2) % n3) * n1 * n2 + (long)((i2 + n2 / 2) % n2) * n1 + (i1 + n1 / 2) % n1] =
+                    creal(S[(long)i3 * n1 * n2 + (long)i2 * n1 + i1]);
+    free(S); free(r.buf1); free(r.buf2);
+    for (int d = 0; d < 3; ++d) plan_free(&r.pl[d]);
+}
+
+/* rotation matrix of Func_rot_3Dvol_FourierShear (inverse = 0) or
+ * Func_inv_rot_3Dvol_FourierShear (inverse = 1); returns 0 when all angles
+ * are within 0.5 degrees (the reference then returns the volume unchanged) */
+int orc_rotation_matrix(const double *v1, const double *v2, const double *v3, double phi, double theta, double psi,
+                        int inverse, double *Mout) {
+    double R1[3][3], R2[3][3], R3[3][3], R[3][3], Rt[3][3];
+    quat_rot(v1, phi, R1);
+    quat_rot(v2, theta, R2);
+    quat_rot(v3, psi, R3);
+    matmul3(R1, R2, R);
+    matmul3(R, R3, R);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Rt[i][j] = R[j][i];
+    if (inverse) inv3(Rt, Rt);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Mout[3 * i + j] = Rt[i][j];
+    return (fabs(theta) > 0.5 || fabs(phi) > 0.5 || fabs(psi) > 0.5) ? 1 : 0;
+}
+
+/* Func_rot_3Dvol_FourierShear / Func_inv_rot_3Dvol_FourierShear with
+ * rotStepInit = 11 (Func_rot_3Dvol_FourierShear.m:15); vol in place (double) */
+int orc_rot3d(double *vol, int n1, int n2, int n3, const double *v1, const double *v2, const double *v3, double phi,
+              double theta, double psi, int inverse) {
+    double M[9];
+    if (!orc_rotation_matrix(v1, v2, v3, phi, theta, psi, inverse, M)) return 0;
+    double MM[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) MM[i][j] = M[3 * i + j];
+    rotate_rotmat(vol, n1, n2, n3, MM, 11.0);
+    return 1;
+}
+
+/* the shear plan of a rotation, for checking a GPU implementation:
+ * out[0] = numStep, out[1] = forward (1) / backward (0), out[2] = mI (1-based),
+ * out[3..10] = coefficients a..h */
+int orc_rotation_plan(const double *M9, double rotStepInit, double *out) {
+    double M[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) M[i][j] = M9[3 * i + j];
+    double qx, qy, qz, qw;
+    quat_from_matrix(M, &qx, &qy, &qz, &qw);
+    double Ang = acos(qw) * 180.0 / M_PI * 2;
+    double nv = sqrt(qx * qx + qy * qy + qz * qz);
+    double Vec[3] = {qx / nv, qy / nv, qz / nv};
+    int numStep = (int)floor(Ang / rotStepInit) + 1;
+    double rotStep = Ang / numStep;
+    double w = cos(rotStep / 2 * M_PI / 180), x = -sin(rotStep / 2 * M_PI / 180) * Vec[0],
+           y = -sin(rotStep / 2 * M_PI / 180) * Vec[1], z = -sin(rotStep / 2 * M_PI / 180) * Vec[2];
+    double cf[3][8], cb[3][8], sf[3], sb[3];
+    for (int i = 1; i <= 3; ++i) {
+        sf[i - 1] = shear_coeffs(x, y, z, w, i, 0, cf[i - 1]);
+        sb[i - 1] = shear_coeffs(x, y, z, w, i, 1, cb[i - 1]);
+    }
+    int mf = 0, mb = 0;
+    for (int i = 1; i < 3; ++i) {
+        if (sf[i] < sf[mf]) mf = i;
+        if (sb[i] < sb[mb]) mb = i;
+    }
+    int fwd = sf[mf] < sb[mb];
+    out[0] = numStep;
+    out[1] = fwd;
+    out[2] = (fwd ? mf : mb) + 1;
+    for (int i = 0; i < 8; ++i) out[3 + i] = fwd ? cf[mf][i] : cb[mb][i];
+    return 0;
+}

@@ -144,3 +144,44 @@ def batched_tilt(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz, binn
 
 def max_threads() -> int:
     return lib().orc_max_threads()
+
+
+def _rot_setup():
+    L = lib()
+    L.orc_rot3d.argtypes = [_D, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int]
+    L.orc_rotation_matrix.argtypes = [_D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int, _D]
+    L.orc_rotation_plan.argtypes = [_D, C.c_double, _D]
+    return L
+
+
+VEC1, VEC2, VEC3 = (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), (1.0, 0.0, 0.0)  # main.m:25-27
+
+
+def rot3d(vol, angles, inverse=False, vecs=(VEC1, VEC2, VEC3)):
+    """Func_rot_3Dvol_FourierShear (inverse=False) / Func_inv_rot_3Dvol_FourierShear
+    (inverse=True) of a C-order [n3][n2][n1] volume (MATLAB size n1 x n2 x n3),
+    FP64.  angles = (phi, theta, psi) in degrees."""
+    L = _rot_setup()
+    v = np.ascontiguousarray(vol, dtype=np.float64).copy()
+    n3, n2, n1 = v.shape
+    vv = [np.asarray(x, dtype=np.float64) for x in vecs]
+    L.orc_rot3d(_d(v), n1, n2, n3, _d(vv[0]), _d(vv[1]), _d(vv[2]), float(angles[0]), float(angles[1]),
+                float(angles[2]), int(inverse))
+    return v
+
+
+def rotation_matrix(angles, inverse=False, vecs=(VEC1, VEC2, VEC3)):
+    L = _rot_setup()
+    vv = [np.asarray(x, dtype=np.float64) for x in vecs]
+    M = np.zeros(9)
+    active = L.orc_rotation_matrix(_d(vv[0]), _d(vv[1]), _d(vv[2]), float(angles[0]), float(angles[1]),
+                                   float(angles[2]), int(inverse), _d(M))
+    return M.reshape(3, 3), bool(active)
+
+
+def rotation_plan(M, step=11.0):
+    L = _rot_setup()
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    out = np.zeros(11)
+    L.orc_rotation_plan(_d(M), float(step), _d(out))
+    return dict(num_step=int(out[0]), forward=bool(out[1]), mI=int(out[2]), coeffs=out[3:].copy())
