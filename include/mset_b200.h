@@ -159,6 +159,39 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 
+/* ---- batched iteration ---------------------------------------------------------
+ * One iteration of the batched method on a cubic lab-frame volume rec (nv^3,
+ * nv == nz, nv <= n, lateral zero-padding to the window):
+ *   V_j  = pad(Func_inv_rot(rec, angles_j))          (STEP01_ROTATION.m:13)
+ *   forward + loss + adjoint of every position of every tilt (one launch)
+ *   rec += step0 * sum_j Func_rot(G_j)                (Run_MSET_recon.m:155, 179)
+ *   positivity (Run_MSET_recon.m:183-185), TV / TV-FISTA of rec / max(rec)
+ *   rescaled by max(rec) (Run_MSET_recon.m:267-270)
+ *   probe_j -= step1 * sum_p shift_{-s}(chi0), positions += step2 * posdir
+ * Every step is stream-ordered on the device; with use_graph the iteration is
+ * captured once as a CUDA graph and replayed. */
+typedef struct {
+    int32_t nv;          /* reconstruction volume edge */
+    const float *angles; /* [ntilts][3] (phi, theta, psi) in degrees (STEM_data.tilt_angles) */
+    const float *vec1, *vec2, *vec3; /* rotation axes (main.m:25-27: [0 0 1], [0 1 0], [1 0 0]) */
+    int32_t use_positivity;
+    int32_t use_tv;
+    double tv_lambda;
+    int32_t tv_iter;
+    int32_t tv_fista; /* 1: TV_FISTA_method, 0: TV_method */
+} mset_iter_args;
+
+int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a);
+/* lab-frame volume in / out: host [nv][nv][nv] float */
+int mset_batch_set_rec(mset_session *s, const float *rec);
+int mset_batch_get_rec(mset_session *s, float *rec);
+/* niter iterations; err_out [niter][ntilts] (sum of (A-M)^2 of the pass before
+ * each update), tv_err_out [niter]; both nullable */
+int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_out, double *tv_err_out);
+/* captures the iteration graph, then times niter replays with CUDA events on
+ * the session stream (the state advances by niter iterations) */
+int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter);
+
 /* ---- Fourier-shear tilt rotation --------------------------------------------
  * Func_rot_3Dvol_FourierShear (inverse = 0) and Func_inv_rot_3Dvol_FourierShear
  * (inverse = 1) (func_lib/Func_rot_3Dvol_FourierShear.m:5-19,

@@ -52,6 +52,11 @@ SIGNATURES = {
     "mset_batch_launch_count": (C.c_int, [C.c_void_p]),
     "mset_rotate_volume": (C.c_int, [C.c_void_p, _F, _F, C.c_int, _F, _F, _F, C.c_double, C.c_double, C.c_double,
                                      C.c_int]),
+    "mset_batch_iteration_setup": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mset_batch_set_rec": (C.c_int, [C.c_void_p, _F]),
+    "mset_batch_get_rec": (C.c_int, [C.c_void_p, _F]),
+    "mset_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D]),
+    "mset_batch_iterate_time": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "mset_tv": (C.c_int, [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D]),
     "mset_batch_gradient_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_float, C.c_float, C.c_int] + [C.c_void_p] * 10),
@@ -97,6 +102,23 @@ class BatchArgs(C.Structure):
         ("ntilts", C.c_int32),
         ("npos", _I),
         ("prop2D", _F),
+    ]
+
+
+class IterArgs(C.Structure):
+    """mset_iter_args (include/mset_b200.h)."""
+
+    _fields_ = [
+        ("nv", C.c_int32),
+        ("angles", _F),
+        ("vec1", _F),
+        ("vec2", _F),
+        ("vec3", _F),
+        ("use_positivity", C.c_int32),
+        ("use_tv", C.c_int32),
+        ("tv_lambda", C.c_double),
+        ("tv_iter", C.c_int32),
+        ("tv_fista", C.c_int32),
     ]
 
 

@@ -108,3 +108,40 @@ class BatchSession:
         ms = np.zeros(1)
         check("mset_batch_time", self._lib.mset_batch_time(self._h, int(reps), dptr(ms)))
         return float(ms[0])
+
+    # ---- full batched iteration -------------------------------------------
+    def iteration_setup(self, nv: int, angles, *, vec1=(0, 0, 1), vec2=(0, 1, 0), vec3=(1, 0, 0),
+                        positivity=True, tv_lambda=0.0, tv_iter=300, tv_fista=True):
+        self._angles = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1, 3))
+        self._vecs = [np.ascontiguousarray(np.asarray(v, dtype=np.float32)) for v in (vec1, vec2, vec3)]
+        a = _lib.IterArgs()
+        a.nv = int(nv)
+        a.angles = fptr(self._angles)
+        a.vec1, a.vec2, a.vec3 = (fptr(v) for v in self._vecs)
+        a.use_positivity = int(bool(positivity))
+        a.use_tv = int(tv_lambda > 0)
+        a.tv_lambda = float(tv_lambda) if tv_lambda > 0 else 1.0
+        a.tv_iter = int(tv_iter)
+        a.tv_fista = int(bool(tv_fista))
+        self.nv = int(nv)
+        check("mset_batch_iteration_setup", self._lib.mset_batch_iteration_setup(self._h, C.byref(a)))
+
+    def set_rec(self, rec):
+        r = _c32(rec)
+        check("mset_batch_set_rec", self._lib.mset_batch_set_rec(self._h, fptr(r)))
+
+    def get_rec(self):
+        r = np.empty((self.nv,) * 3, np.float32)
+        check("mset_batch_get_rec", self._lib.mset_batch_get_rec(self._h, fptr(r)))
+        return r
+
+    def iterate(self, niter: int, use_graph: bool = True):
+        e = np.zeros((max(niter, 1), self.ntilts))
+        t = np.zeros(max(niter, 1))
+        check("mset_batch_iterate", self._lib.mset_batch_iterate(self._h, int(niter), int(use_graph), dptr(e), dptr(t)))
+        return e[:niter], t[:niter]
+
+    def time_iteration(self, niter: int) -> float:
+        ms = np.zeros(1)
+        check("mset_batch_iterate_time", self._lib.mset_batch_iterate_time(self._h, int(niter), dptr(ms)))
+        return float(ms[0])

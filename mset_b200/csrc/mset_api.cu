@@ -111,6 +111,20 @@ struct mset_session {
     int save_slots = 0;
     std::vector<TiltDev> h_tilts;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // batched iteration (rotate -> pass -> rotate back -> update -> TV)
+    bool it_ready = false;
+    int nv = 0;
+    std::vector<RotPlan> plan_inv, plan_fwd;
+    DevBuf<float> rec, gvol;
+    DevBuf<double> gacc, err_hist, tv_hist;
+    DevBuf<unsigned> it_counter, mx_bits;
+    DevBuf<float> mx;
+    int it_pos = 1, it_tv = 0, it_tv_iter = 0, it_tv_fista = 1;
+    double it_tv_lambda = 0;
+    int hist_cap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int grid_cache = 0;
     // TV work buffers
     DevBuf<float> tv_in, tv_out, tv_P, tv_Y, tv_D;
     DevBuf<double> tv_err;
@@ -344,6 +358,8 @@ int mset_destroy(mset_session *s) {
     if (!s) return 0;
     cudaSetDevice(s->device);
     if (s->st) cudaStreamSynchronize(s->st);
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
     s->tilts.clear();
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -785,6 +801,217 @@ int mset_tv(mset_session *s, float *vol, int n1, int n2, int n3, double lambda, 
     CK(cudaMemcpyAsync(&e, s->tv_err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if (tv_error) *tv_error = e;
+    return 0;
+}
+
+// ---- batched iteration ------------------------------------------------------
+static void drop_graph(mset_session *s) {
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->graph_exec = nullptr;
+    s->graph = nullptr;
+}
+
+namespace {
+// history slot: hist[k * J + j] = err[j], k from a device counter, so the
+// same captured graph appends on every replay
+__global__ void k_record_err(const double *err, int J, double *hist, int cap, unsigned *counter, const double *tv_err,
+                             double *tv_hist) {
+    const unsigned k = *counter;
+    if (k < (unsigned)cap) {
+        for (int j = threadIdx.x; j < J; j += blockDim.x) hist[(size_t)k * J + j] = err[j];
+        if (threadIdx.x == 0 && tv_err) tv_hist[k] = *tv_err;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = k + 1;
+}
+}  // namespace
+
+int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!a || !a->angles || !a->vec1 || !a->vec2 || !a->vec3) return fail(MSET_E_ARG, "null argument");
+    const int nv = a->nv;
+    if (nv != s->nz) return fail(MSET_E_ARG, "the reconstruction edge nv (%d) must equal the depth nz (%d)", nv, s->nz);
+    if (nv > s->n) return fail(MSET_E_ARG, "the reconstruction edge nv (%d) exceeds the window (%d)", nv, s->n);
+    if ((s->n - nv) % 2) return fail(MSET_E_ARG, "window minus volume edge must be even (centred padding)");
+    if (a->use_tv && (!(a->tv_lambda > 0) || a->tv_iter < 0)) return fail(MSET_E_ARG, "bad TV parameters");
+    rc = rot_prepare(s, nv);
+    if (rc) return rc;
+    const int J = (int)s->tilts.size();
+    const double v1[3] = {a->vec1[0], a->vec1[1], a->vec1[2]}, v2[3] = {a->vec2[0], a->vec2[1], a->vec2[2]},
+                 v3[3] = {a->vec3[0], a->vec3[1], a->vec3[2]};
+    s->plan_inv.resize(J);
+    s->plan_fwd.resize(J);
+    for (int j = 0; j < J; ++j) {
+        const float *an = a->angles + 3 * j;
+        rot_plan(v1, v2, v3, an[0], an[1], an[2], true, &s->plan_inv[j]);   // Func_inv_rot (STEP01_ROTATION.m:13)
+        rot_plan(v1, v2, v3, an[0], an[1], an[2], false, &s->plan_fwd[j]);  // Func_rot (Run_MSET_recon.m:179)
+    }
+    const size_t V = (size_t)nv * nv * nv;
+    CK(s->rec.ensure(V));
+    CK(s->gvol.ensure(V));
+    CK(s->gacc.ensure(V));
+    CK(s->it_counter.ensure(1));
+    CK(s->mx_bits.ensure(1));
+    CK(s->mx.ensure(1));
+    CK(cudaMemsetAsync(s->rec.p, 0, sizeof(float) * V, s->st));
+    s->nv = nv;
+    s->it_pos = a->use_positivity ? 1 : 0;
+    s->it_tv = a->use_tv ? 1 : 0;
+    s->it_tv_iter = a->tv_iter;
+    s->it_tv_fista = a->tv_fista ? 1 : 0;
+    s->it_tv_lambda = a->tv_lambda;
+    if (s->it_tv) {
+        CK(s->tv_in.ensure(V));
+        CK(s->tv_out.ensure(V));
+        CK(s->tv_P.ensure(3 * V));
+        CK(s->tv_Y.ensure(3 * V));
+        CK(s->tv_D.ensure(V));
+        CK(s->tv_err.ensure(1));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    drop_graph(s);
+    s->it_ready = true;
+    return 0;
+}
+
+int mset_batch_set_rec(mset_session *s, const float *rec) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (!rec) return fail(MSET_E_ARG, "null volume");
+    CK(cudaMemcpyAsync(s->rec.p, rec, sizeof(float) * (size_t)s->nv * s->nv * s->nv, cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_get_rec(mset_session *s, float *rec) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (!rec) return fail(MSET_E_ARG, "null volume");
+    CK(cudaMemcpyAsync(rec, s->rec.p, sizeof(float) * (size_t)s->nv * s->nv * s->nv, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+// everything of one iteration, stream-ordered, no host synchronisation and
+// no pageable copies: safe to capture into a CUDA graph
+static int record_iteration(mset_session *s) {
+    const int J = (int)s->tilts.size();
+    const int nv = s->nv, n = s->n;
+    const long V = (long)nv * nv * nv;
+    const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
+    const int bvox = s->method == MSET_MODE_SSET ? s->nz : s->b;
+    const size_t n2 = (size_t)n * n;
+    // 1. beam-frame volumes V_j = pad(Func_inv_rot(rec, angles_j))
+    for (int j = 0; j < J; ++j) {
+        CKL(rot_apply(s->plan_inv[j], nv, s->rec.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
+        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, nv, n, s->st), "pad");
+    }
+    // 2. the batched pass over all positions of all tilts
+    for (auto &t : s->tilts) {
+        CK(cudaMemsetAsync(t.grad.p, 0, sizeof(double) * n2 * nsg, s->st));
+        CK(cudaMemsetAsync(t.qacc.p, 0, sizeof(double) * n2 * 2, s->st));
+    }
+    CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * J, s->st));
+    CKL(launch_transmission(s->d_tilts.p, J, n, s->nz, bvox, nsg, s->sigma * s->dz, s->st), "transmission");
+    CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
+    LaunchArgs la = base_args(s);
+    CKL(launch_positions(s->plan, s->method, s->adjoint, kBatch, la, s->grid_cache, s->st), "position kernel");
+    // 3. gradient back to the lab frame: sum_j Func_rot(G_j)
+    for (int j = 0; j < J; ++j) {
+        CKL(vol_slab_to_volume(s->tilts[j].grad.p, s->gvol.p, nv, n, bvox, s->st), "slab_to_volume");
+        CKL(rot_apply(s->plan_fwd[j], nv, s->gvol.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
+        CKL(vol_accumulate(s->gvol.p, s->gacc.p, V, j == 0, s->st), "accumulate");
+    }
+    // 4. object update, positivity (Run_MSET_recon.m:183-185), TV (:267-270)
+    CKL(vol_update(s->rec.p, s->gacc.p, V, s->step[0], s->st), "update");
+    if (s->it_pos) CKL(vol_positivity(s->rec.p, V, s->st), "positivity");
+    if (s->it_tv) {
+        CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
+        CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
+        CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
+        TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
+                  s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
+        CKL(tv_prox(ta, s->st), "tv");
+        CKL(vol_mul(s->tv_out.p, s->rec.p, V, s->mx.p, s->st), "rescale");
+    }
+    // 5. probe and scan positions
+    CKL(launch_apply_probe_pos(s->h_tilts.data(), J, n, s->step[1], s->step[2], s->st), "apply");
+    // 6. error history
+    k_record_err<<<1, 64, 0, s->st>>>(s->err.p, J, s->err_hist.p, s->hist_cap, s->it_counter.p,
+                                      s->it_tv ? s->tv_err.p : nullptr, s->tv_hist.p);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_out, double *tv_err_out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (niter < 0) return fail(MSET_E_ARG, "niter < 0");
+    const int J = (int)s->tilts.size();
+    // everything that allocates or copies from the host happens here, before
+    // the iterations (and before any capture)
+    const int grid = persistent_grid(s, std::max(1, s->total_pos));
+    rc = ensure_save(s, grid);
+    if (rc) return rc;
+    s->grid_cache = grid;
+    rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    const int cap = std::max(1, niter);
+    if (s->hist_cap < cap) {
+        CK(s->err_hist.ensure((size_t)cap * J));
+        CK(s->tv_hist.ensure(cap));
+        s->hist_cap = cap;
+        drop_graph(s);
+    }
+    CK(cudaMemsetAsync(s->it_counter.p, 0, sizeof(unsigned), s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (use_graph) {
+        if (!s->graph_exec) {
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
+            rc = record_iteration(s);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(s->st, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+            s->graph = g;
+            CK(cudaGraphInstantiate(&s->graph_exec, g, 0));
+        }
+        for (int k = 0; k < niter; ++k) CK(cudaGraphLaunch(s->graph_exec, s->st));
+    } else {
+        for (int k = 0; k < niter; ++k) {
+            rc = record_iteration(s);
+            if (rc) return rc;
+        }
+    }
+    if (err_out && niter)
+        CK(cudaMemcpyAsync(err_out, s->err_hist.p, sizeof(double) * niter * J, cudaMemcpyDeviceToHost, s->st));
+    if (tv_err_out && niter)
+        CK(cudaMemcpyAsync(tv_err_out, s->tv_hist.p, sizeof(double) * niter, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!ms_per_iter || niter <= 0) return fail(MSET_E_ARG, "bad arguments");
+    rc = mset_batch_iterate(s, 1, 1, nullptr, nullptr);  // capture + one replay
+    if (rc) return rc;
+    CK(cudaEventRecord(s->ev0, s->st));
+    for (int k = 0; k < niter; ++k) CK(cudaGraphLaunch(s->graph_exec, s->st));
+    CK(cudaEventRecord(s->ev1, s->st));
+    CK(cudaEventSynchronize(s->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *ms_per_iter = ms / niter;
     return 0;
 }
 

@@ -116,4 +116,13 @@ int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, fl
     return (int)cudaGetLastError();
 }
 
+int launch_apply_probe_pos(const TiltDev *tilts, int ntilts, int n, float step1, float step2, cudaStream_t st) {
+    for (int j = 0; j < ntilts; ++j) {
+        const TiltDev &t = tilts[j];
+        k_apply_probe<<<64, 256, 0, st>>>(t.Q, t.qacc, n * n, step1);
+        if (t.npos) k_apply_pos<<<8, 256, 0, st>>>(t.sx, t.sy, t.posdir, t.npos, step2);
+    }
+    return (int)cudaGetLastError();
+}
+
 }  // namespace mset

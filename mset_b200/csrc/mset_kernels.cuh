@@ -76,6 +76,7 @@ int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const floa
 // thread-local error message of the C ABI (mset_last_error)
 void set_last_error(const char *msg);
 
+int launch_apply_probe_pos(const TiltDev *tilts_host, int ntilts, int n, float step1, float step2, cudaStream_t st);
 int launch_transmission(const TiltDev *tilts_dev, int ntilts, int n, int nz, int b, int ns, float sdz,
                         cudaStream_t st);
 int launch_apply_batch(int n, int nz, int b, int ns, int method, float step0, float step1, float step2,

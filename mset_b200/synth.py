@@ -149,6 +149,7 @@ class Specimen:
     cfg: Config
     angles: np.ndarray        # [J, 3]
     volumes: list             # per tilt beam-frame volume [nz][n][n] float32 (ground truth)
+    lab: np.ndarray | None    # lab-frame volume [nz][ny][nx] float32 (ground truth, unpadded)
     probe: np.ndarray         # [n][n] complex64, normalised to the dose
     prop: np.ndarray          # [n][n] complex64 centred
     scan_x: np.ndarray        # [P] float32
@@ -165,7 +166,9 @@ def make_specimen(cfg: Config, with_volumes: bool = True) -> Specimen:
     pos, peak = atoms(cfg, rng)
     angles = tilt_angles(cfg)
     vols = []
+    lab = None
     if with_volumes:
+        lab = voxelise(pos, peak, cfg.vol, cfg.dx, cfg.blob_sigma).astype(np.float32)
         for th in angles[:, 1]:
             # beam frame of tilt th: the reference's Func_inv_rot_3Dvol_FourierShear
             # with (phi, theta, psi) = (0, th, 0) maps (x, 0, 0) to (x cos th, 0, x sin th)
@@ -177,7 +180,7 @@ def make_specimen(cfg: Config, with_volumes: bool = True) -> Specimen:
     probe = physics.normalise_probe(probe, cfg.dose).astype(np.complex64)
     prop = physics.propagator(n, cfg.dx, lam, cfg.slice_binning)
     sx, sy = raster(cfg, rng)
-    return Specimen(cfg, angles, vols, probe, prop, sx, sy, float(sigma), float(lam), len(pos))
+    return Specimen(cfg, angles, vols, lab, probe, prop, sx, sy, float(sigma), float(lam), len(pos))
 
 
 def poisson(intensities: np.ndarray, seed: int) -> np.ndarray:
