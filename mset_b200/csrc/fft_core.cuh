@@ -271,7 +271,9 @@ __device__ __forceinline__ void sync_cols() {
 }
 __device__ __forceinline__ void sync_all() { __syncthreads(); }
 
-struct NoPre {};
+struct NoPre {
+    static constexpr bool kAhead = false;
+};
 
 // Row pass A.  Task (y, n1) owns x = n1 + R1*j, j < R2.
 //   pf(y, n1, pre) : issue the global loads the op needs (before the shared
@@ -285,11 +287,19 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
     constexpr int R1 = G::R1, R2 = G::R2;
     constexpr int TASKS = O::RPW * R1;
     const int y0 = O::warp() * O::RPW;
+    // Pre::kAhead: issue the next task's global loads while the current task
+    // runs (double-buffered prefetch); otherwise just before its shared reads
+    constexpr bool ahead = Pre::kAhead;
+    Pre pre, nxt;
+    if (ahead && O::lane() < TASKS) pf(y0 + O::lane() / R1, O::lane() % R1, pre);
 #pragma unroll 1
     for (int tau = O::lane(); tau < TASKS; tau += 32) {
         const int n1 = tau % R1, y = y0 + tau / R1;
-        Pre pre;
-        pf(y, n1, pre);
+        if constexpr (ahead) {
+            if (tau + 32 < TASKS) pf(y0 + (tau + 32) / R1, (tau + 32) % R1, nxt);
+        } else {
+            pf(y, n1, pre);
+        }
         float2 *row = buf + y * G::S + n1;
         float2 v[R2];
 #pragma unroll
@@ -307,6 +317,7 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
         }
 #pragma unroll
         for (int j = 0; j < R2; ++j) row[(R1 + 1) * j] = v[j];
+        if constexpr (ahead) pre = nxt;
     }
 }
 

@@ -77,10 +77,12 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
 
 template <class G>
 struct TPre {
+    static constexpr bool kAhead = true;
     float2 t[G::R2];  // transmission of the task's elements
 };
 template <class G>
 struct TSPre {
+    static constexpr bool kAhead = false;  // two operands: no room for a second buffer
     float2 t[G::R2];  // transmission
     float2 w[G::R2];  // saved wave
 };
@@ -445,15 +447,21 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     float2 *buf = smem;
     double *red = reinterpret_cast<double *>(buf + Smem<G>::END);
     __shared__ int s_item;
+    // the tilt's descriptor lives in shared memory for the whole position:
+    // its pointers are read on every pass, and a global read of them would
+    // sit in front of every dependent load
+    __shared__ TiltDev s_tilt;
     load_tables<G>(buf, a);
     const int nsave = (METHOD == kSSET ? 1 : a.ns) + 1;
     float2 *save = a.save + (size_t)blockIdx.x * nsave * G::N * G::N;
     __syncthreads();
     using K = PositionKernel<G, METHOD, ADJ, MODE>;
     if constexpr (MODE == kSeq) {
-        const TiltDev &t = a.tilts[a.seq_tilt];
-        for (int p = 0; p < t.npos; ++p) K::run(a, t, p, buf, save, red);
+        if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
+        __syncthreads();
+        for (int p = 0; p < s_tilt.npos; ++p) K::run(a, s_tilt, p, buf, save, red);
     } else {
+        int cur = -1;
         for (;;) {
             if (threadIdx.x == 0) s_item = (int)atomicAdd(a.counter, 1u);
             __syncthreads();
@@ -461,7 +469,12 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
             __syncthreads();
             if (it >= a.nitems) break;
             const int2 tp = a.items[it];
-            K::run(a, a.tilts[tp.x], tp.y, buf, save, red);
+            if (tp.x != cur) {
+                if (threadIdx.x == 0) s_tilt = a.tilts[tp.x];
+                __syncthreads();
+                cur = tp.x;
+            }
+            K::run(a, s_tilt, tp.y, buf, save, red);
         }
     }
 }
