@@ -175,7 +175,24 @@ def run_ours(args):
         bs.iteration_setup(cfg.vol[0], spec.angles, positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter,
                            tv_fista=True)
         bs.set_rec(0.5 * spec.lab)
-        it_ms = bs.time_iteration(max(1, min(args.steps, 3)))
+        k_it = max(1, min(args.steps, 3))
+        if world == 1:
+            it_ms = bs.time_iteration(k_it)
+        else:
+            # tilts sharded over ranks: one NCCL all-reduce of the FP64
+            # lab-frame gradient per iteration, on the session stream
+            from mset_b200.distributed import GpuBackend, sharded_iterate
+            be = GpuBackend(bs)
+            sharded_iterate(be, 1)  # capture both phase graphs (warm-up)
+            torch.cuda.synchronize()
+            dist.barrier()
+            with be.stream():
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                sharded_iterate(be, k_it)
+                e1.record()
+            e1.synchronize()
+            it_ms = e0.elapsed_time(e1) / k_it
         t = torch.tensor([it_ms], dtype=torch.float64, device=f"cuda:{local}")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)

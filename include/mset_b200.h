@@ -191,6 +191,15 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
 /* captures the iteration graph, then times niter replays with CUDA events on
  * the session stream (the state advances by niter iterations) */
 int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter);
+/* one phase of an iteration, for tilt sharding over GPUs: phase 1 ends with
+ * this session's lab-frame gradient sum in the FP64 device buffer of
+ * mset_batch_device_info; the caller all-reduces it (NCCL, on the session
+ * stream) and runs phase 2, the update.  Asynchronous on the session stream. */
+int mset_batch_iterate_phase(mset_session *s, int phase, int use_graph);
+/* device buffers and stream of the iteration: gacc [nv^3] double, the session
+ * cudaStream_t, the per-tilt error sums [ntilts] double; any pointer may be NULL */
+int mset_batch_device_info(mset_session *s, void **gacc_dev, size_t *gacc_count, void **stream,
+                           double **err_dev);
 
 /* ---- Fourier-shear tilt rotation --------------------------------------------
  * Func_rot_3Dvol_FourierShear (inverse = 0) and Func_inv_rot_3Dvol_FourierShear

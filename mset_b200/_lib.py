@@ -57,6 +57,9 @@ SIGNATURES = {
     "mset_batch_get_rec": (C.c_int, [C.c_void_p, _F]),
     "mset_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D]),
     "mset_batch_iterate_time": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "mset_batch_iterate_phase": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "mset_batch_device_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                                         C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "mset_tv": (C.c_int, [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D]),
     "mset_batch_gradient_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_float, C.c_float, C.c_int] + [C.c_void_p] * 10),

@@ -124,6 +124,8 @@ struct mset_session {
     int hist_cap = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    cudaGraph_t phase_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t phase_exec[2] = {nullptr, nullptr};
     int grid_cache = 0;
     // TV work buffers
     DevBuf<float> tv_in, tv_out, tv_P, tv_Y, tv_D;
@@ -360,6 +362,10 @@ int mset_destroy(mset_session *s) {
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
     if (s->graph) cudaGraphDestroy(s->graph);
+    for (int p = 0; p < 2; ++p) {
+        if (s->phase_exec[p]) cudaGraphExecDestroy(s->phase_exec[p]);
+        if (s->phase_graph[p]) cudaGraphDestroy(s->phase_graph[p]);
+    }
     s->tilts.clear();
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -810,6 +816,12 @@ static void drop_graph(mset_session *s) {
     if (s->graph) cudaGraphDestroy(s->graph);
     s->graph_exec = nullptr;
     s->graph = nullptr;
+    for (int p = 0; p < 2; ++p) {
+        if (s->phase_exec[p]) cudaGraphExecDestroy(s->phase_exec[p]);
+        if (s->phase_graph[p]) cudaGraphDestroy(s->phase_graph[p]);
+        s->phase_exec[p] = nullptr;
+        s->phase_graph[p] = nullptr;
+    }
 }
 
 namespace {
@@ -897,14 +909,18 @@ int mset_batch_get_rec(mset_session *s, float *rec) {
 }
 
 // everything of one iteration, stream-ordered, no host synchronisation and
-// no pageable copies: safe to capture into a CUDA graph
-static int record_iteration(mset_session *s) {
+// no pageable copies: safe to capture into a CUDA graph.  Phase 1: beam-frame
+// volumes, the batched pass and the lab-frame gradient sum over this
+// session's tilts (gacc); phase 2: the update from gacc.  A caller that
+// shards tilts over GPUs all-reduces gacc between the phases.
+static int record_phase(mset_session *s, int phase) {
     const int J = (int)s->tilts.size();
     const int nv = s->nv, n = s->n;
     const long V = (long)nv * nv * nv;
     const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
     const int bvox = s->method == MSET_MODE_SSET ? s->nz : s->b;
     const size_t n2 = (size_t)n * n;
+    if (phase == 2) goto update;
     // 1. beam-frame volumes V_j = pad(Func_inv_rot(rec, angles_j))
     for (int j = 0; j < J; ++j) {
         CKL(rot_apply(s->plan_inv[j], nv, s->rec.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
@@ -918,14 +934,18 @@ static int record_iteration(mset_session *s) {
     CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * J, s->st));
     CKL(launch_transmission(s->d_tilts.p, J, n, s->nz, bvox, nsg, s->sigma * s->dz, s->st), "transmission");
     CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
-    LaunchArgs la = base_args(s);
-    CKL(launch_positions(s->plan, s->method, s->adjoint, kBatch, la, s->grid_cache, s->st), "position kernel");
+    {
+        LaunchArgs la = base_args(s);
+        CKL(launch_positions(s->plan, s->method, s->adjoint, kBatch, la, s->grid_cache, s->st), "position kernel");
+    }
     // 3. gradient back to the lab frame: sum_j Func_rot(G_j)
     for (int j = 0; j < J; ++j) {
         CKL(vol_slab_to_volume(s->tilts[j].grad.p, s->gvol.p, nv, n, bvox, s->st), "slab_to_volume");
         CKL(rot_apply(s->plan_fwd[j], nv, s->gvol.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
         CKL(vol_accumulate(s->gvol.p, s->gacc.p, V, j == 0, s->st), "accumulate");
     }
+    if (phase == 1) return 0;
+update:
     // 4. object update, positivity (Run_MSET_recon.m:183-185), TV (:267-270)
     CKL(vol_update(s->rec.p, s->gacc.p, V, s->step[0], s->st), "update");
     if (s->it_pos) CKL(vol_positivity(s->rec.p, V, s->st), "positivity");
@@ -933,7 +953,7 @@ static int record_iteration(mset_session *s) {
         CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
         CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
         CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
-        TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
+        const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
                   s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
         CKL(tv_prox(ta, s->st), "tv");
         CKL(vol_mul(s->tv_out.p, s->rec.p, V, s->mx.p, s->st), "rescale");
@@ -973,7 +993,8 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
     if (use_graph) {
         if (!s->graph_exec) {
             CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
-            rc = record_iteration(s);
+            rc = record_phase(s, 1);
+            if (!rc) rc = record_phase(s, 2);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(s->st, &g);
             if (rc) {
@@ -987,7 +1008,8 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
         for (int k = 0; k < niter; ++k) CK(cudaGraphLaunch(s->graph_exec, s->st));
     } else {
         for (int k = 0; k < niter; ++k) {
-            rc = record_iteration(s);
+            rc = record_phase(s, 1);
+            if (!rc) rc = record_phase(s, 2);
             if (rc) return rc;
         }
     }
@@ -996,6 +1018,71 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
     if (tv_err_out && niter)
         CK(cudaMemcpyAsync(tv_err_out, s->tv_hist.p, sizeof(double) * niter, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+static void drop_phase_graphs(mset_session *s) {
+    for (int p = 0; p < 2; ++p) {
+        if (s->phase_exec[p]) cudaGraphExecDestroy(s->phase_exec[p]);
+        if (s->phase_graph[p]) cudaGraphDestroy(s->phase_graph[p]);
+        s->phase_exec[p] = nullptr;
+        s->phase_graph[p] = nullptr;
+    }
+}
+
+int mset_batch_iterate_phase(mset_session *s, int phase, int use_graph) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (phase != 1 && phase != 2) return fail(MSET_E_ARG, "phase must be 1 or 2");
+    if (phase == 1 || !s->grid_cache) {
+        const int grid = persistent_grid(s, std::max(1, s->total_pos));
+        rc = ensure_save(s, grid);
+        if (rc) return rc;
+        if (grid != s->grid_cache) drop_phase_graphs(s);
+        s->grid_cache = grid;
+        rc = refresh_tilt_table(s);
+        if (rc) return rc;
+        if (s->hist_cap < 1) {
+            CK(s->err_hist.ensure(s->tilts.size()));
+            CK(s->tv_hist.ensure(1));
+            s->hist_cap = 1;
+        }
+    }
+    // the history slot of a single phase call is always the first
+    CK(cudaMemsetAsync(s->it_counter.p, 0, sizeof(unsigned), s->st));
+    if (use_graph) {
+        cudaGraphExec_t &ex = s->phase_exec[phase - 1];
+        if (!ex) {
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
+            rc = record_phase(s, phase);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(s->st, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+            s->phase_graph[phase - 1] = g;
+            CK(cudaGraphInstantiate(&ex, g, 0));
+        }
+        CK(cudaGraphLaunch(ex, s->st));
+    } else {
+        rc = record_phase(s, phase);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int mset_batch_device_info(mset_session *s, void **gacc_dev, size_t *gacc_count, void **stream,
+                           double **err_dev) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (gacc_dev) *gacc_dev = s->gacc.p;
+    if (gacc_count) *gacc_count = (size_t)s->nv * s->nv * s->nv;
+    if (stream) *stream = (void *)s->st;
+    if (err_dev) *err_dev = s->err.p;
     return 0;
 }
 
