@@ -159,6 +159,12 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 
+/* checkpointing of the batched pass: keep the wave entering every k-th slab
+ * and recompute a segment's waves right before its adjoint (one extra forward
+ * per slab, (ceil(ns/k) + k + 2) instead of (ns + 1) saved n x n waves per
+ * resident CTA); k = 0 or k >= ns keeps every wave */
+int mset_batch_set_checkpoint(mset_session *s, int k);
+
 /* ---- batched iteration ---------------------------------------------------------
  * One iteration of the batched method on a cubic lab-frame volume rec (nv^3,
  * nv == nz, nv <= n, lateral zero-padding to the window):

@@ -109,6 +109,11 @@ class BatchSession:
         check("mset_batch_time", self._lib.mset_batch_time(self._h, int(reps), dptr(ms)))
         return float(ms[0])
 
+    def set_checkpoint(self, k: int):
+        """keep the wave entering every k-th slab and recompute the rest in the
+        adjoint (0: keep all)"""
+        check("mset_batch_set_checkpoint", self._lib.mset_batch_set_checkpoint(self._h, int(k)))
+
     # ---- full batched iteration -------------------------------------------
     def iteration_setup(self, nv: int, angles, *, vec1=(0, 0, 1), vec2=(0, 1, 0), vec3=(1, 0, 0),
                         positivity=True, tv_lambda=0.0, tv_iter=300, tv_fista=True):

@@ -109,6 +109,7 @@ struct mset_session {
     DevBuf<unsigned> counter;
     DevBuf<float> inten;
     int save_slots = 0;
+    int ckpt = 0;  // checkpoint interval of the batched pass (0: keep every wave)
     std::vector<TiltDev> h_tilts;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // batched iteration (rotate -> pass -> rotate back -> update -> TV)
@@ -226,8 +227,8 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
 }
 
 int ensure_save(mset_session *s, int slots) {
-    const size_t per = (size_t)(s->ns + 1) * s->n * s->n;
-    if (s->save_slots >= slots && s->save.n >= per * slots) return 0;
+    const size_t per = (size_t)save_slots(s->ns, s->ckpt) * s->n * s->n;
+    if (s->save.n >= per * slots) return 0;
     cudaError_t e = s->save.ensure(per * slots);
     if (e != cudaSuccess) return cuda_fail(e, "allocating saved-wave buffers");
     s->save_slots = slots;
@@ -306,10 +307,13 @@ LaunchArgs base_args(mset_session *s) {
     a.step1 = s->step[1];
     a.step2 = s->step[2];
     a.seq_tilt = 0;
+    a.ckpt = s->ckpt;
+    a.slots = save_slots(s->ns, s->ckpt);
     return a;
 }
 
 int launch_queue(mset_session *s, int method, int adjoint, int mode) {
+    if (mode == kBatch && method == kMSET && s->ckpt > 0 && s->ckpt < s->ns) mode = kBatchCk;
     const int grid = persistent_grid(s, s->total_pos);
     int rc = ensure_save(s, grid);
     if (rc) return rc;
@@ -936,7 +940,8 @@ static int record_phase(mset_session *s, int phase) {
     CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
     {
         LaunchArgs la = base_args(s);
-        CKL(launch_positions(s->plan, s->method, s->adjoint, kBatch, la, s->grid_cache, s->st), "position kernel");
+        const int mode = (s->method == kMSET && s->ckpt > 0 && s->ckpt < s->ns) ? kBatchCk : kBatch;
+        CKL(launch_positions(s->plan, s->method, s->adjoint, mode, la, s->grid_cache, s->st), "position kernel");
     }
     // 3. gradient back to the lab frame: sum_j Func_rot(G_j)
     for (int j = 0; j < J; ++j) {
@@ -1099,6 +1104,16 @@ int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_iter = ms / niter;
+    return 0;
+}
+
+int mset_batch_set_checkpoint(mset_session *s, int k) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (k < 0) return fail(MSET_E_ARG, "checkpoint interval must be >= 0");
+    s->ckpt = k;
+    s->grid_cache = 0;
+    drop_graph(s);
     return 0;
 }
 

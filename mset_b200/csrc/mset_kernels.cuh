@@ -14,7 +14,8 @@ enum Mode {
     kBatch = 1,  // fixed state, accumulate FP64 gradients over positions
     kErr = 2,    // forward + error only (run_error_mset / run_error_sset)
     kSim = 3,    // forward + write |Psi|^2 (centred layout)
-    kBatchCentred = 4  // kBatch reading the caller's centred intensities (no prepared amplitudes)
+    kBatchCentred = 4,  // kBatch reading the caller's centred intensities (no prepared amplitudes)
+    kBatchCk = 5        // kBatch keeping every k-th wave and recomputing the rest (checkpointing)
 };
 
 // one tilt: all buffers on the device
@@ -47,7 +48,16 @@ struct LaunchArgs {
     float center;           // round((N+1)/2)
     float step0, step1, step2;
     int seq_tilt;           // kSeq: index of the tilt to run
+    int ckpt;               // 0: keep every slab's wave; k: keep every k-th, recompute the rest
+    int slots;              // saved-wave slots (n x n complex) per CTA
 };
+
+// saved-wave slots a CTA needs for ns slabs with checkpoint interval k
+__host__ __device__ inline int save_slots(int ns, int k) {
+    if (k <= 0 || k >= ns) return ns + 1;
+    const int nseg = (ns + k - 1) / k;
+    return nseg + k + 2;  // checkpoints, recomputed waves of a segment, parked adjoint state
+}
 
 // per-window-size kernel table (one translation unit per size, geo_<N>.cu)
 struct GeoOps {

@@ -141,6 +141,62 @@ struct PositionKernel {
         return __ldg(a.pscr + (size_t)Ly * N + Lx);
     }
 
+    // forward through slabs s0 .. s1-1 from the checkpointed wave entering s0,
+    // storing the wave after slab s at out[s - s0] (mset.cu:157-183)
+    static __device__ __noinline__ void recompute(const LaunchArgs &a, const TiltDev &t, int s0, int s1, float2 *buf,
+                                     const float2 *tw, const float2 *py, const float2 *px, const float2 *ckw,
+                                     float2 *out) {
+        row_passA_pf<G, 0, -1, TPre<G>>(
+            buf, tw,
+            [&](int y, int n1, TPre<G> &pre) {
+#pragma unroll
+                for (int j = 0; j < R2; ++j) pre.t[j] = trans(a, t, s0, y, n1 + R1 * j);
+            },
+            [&](int y, int n1, float2 *v, const TPre<G> &pre) {
+                const float2 *w = ckw + (size_t)y * N + n1;
+#pragma unroll
+                for (int j = 0; j < R2; ++j) v[j] = cmul(w[R1 * j], pre.t[j]);
+            });
+        sync_rows();
+        for (int s = s0; s < s1; ++s) {
+            row_passB<G, -1>(buf);
+            sync_all();
+            col_passA<G, -1, true>(buf, tw);
+            sync_cols<G>();
+            col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+                for (int j = 0; j < R1; ++j) v[j] = cmul(v[j], prop(a, py, px, y0 + j, x));
+            });
+            sync_cols<G>();
+            col_passA<G, +1, false>(buf, tw);
+            sync_all();
+            row_passB<G, +1>(buf);
+            sync_rows();
+            float2 *o = out + (size_t)(s - s0) * NN;
+            auto store = [&](int y, int n1, float2 *v) {
+                float2 *w = o + (size_t)y * N + n1;
+#pragma unroll
+                for (int j = 0; j < R2; ++j) w[R1 * j] = v[j];
+            };
+            if (s + 1 < s1) {
+                row_passA_pf<G, +1, -1, TPre<G>>(
+                    buf, tw,
+                    [&](int y, int n1, TPre<G> &pre) {
+#pragma unroll
+                        for (int j = 0; j < R2; ++j) pre.t[j] = trans(a, t, s + 1, y, n1 + R1 * j);
+                    },
+                    [&](int y, int n1, float2 *v, const TPre<G> &pre) {
+                        store(y, n1, v);
+#pragma unroll
+                        for (int j = 0; j < R2; ++j) v[j] = cmul(v[j], pre.t[j]);
+                    });
+            } else {
+                row_passA<G, +1, 0>(buf, tw, store);
+            }
+            sync_rows();
+        }
+    }
+
     static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, float2 *save,
                                double *red) {
         const float2 *tw = buf + Smem<G>::TW;
@@ -149,6 +205,12 @@ struct PositionKernel {
         const float2 *py = buf + Smem<G>::PY;
         const float2 *px = buf + Smem<G>::PX;
         const int ns = METHOD == kSSET ? 1 : a.ns;
+        // checkpointing: keep the wave entering every k-th slab, recompute the
+        // waves of a segment right before its adjoint (k = 0: keep them all)
+        const int ck = (MODE == kBatchCk && a.ckpt > 0 && a.ckpt < ns) ? a.ckpt : 0;
+        const int nseg = ck ? (ns + ck - 1) / ck : 1;
+        float2 *recbuf = save + (size_t)nseg * NN;
+        float2 *park = save + (size_t)(nseg + ck) * NN;
         float *V = t.V;
         const float sxp = t.sx[p], syp = t.sy[p];
         const float s1 = syp - a.center, s2 = sxp - a.center;  // mset.cu:121
@@ -219,9 +281,15 @@ struct PositionKernel {
                     },
                     [&](int y, int n1, float2 *v, const TPre<G> &pre) {
                         if constexpr (MODE != kSim && MODE != kErr) {
-                            float2 *sv = save + (size_t)(s + 1) * NN + (size_t)y * N + n1;
+                            const int w = s + 1;
+                            float2 *sv = nullptr;
+                            if (!ck) sv = save + (size_t)w * NN;
+                            else if (w % ck == 0 && w < ns) sv = save + (size_t)(w / ck) * NN;
+                            if (sv) {
+                                sv += (size_t)y * N + n1;
 #pragma unroll
-                            for (int j = 0; j < R2; ++j) sv[R1 * j] = v[j];
+                                for (int j = 0; j < R2; ++j) sv[R1 * j] = v[j];
+                            }
                         }
                         if (!last) {
 #pragma unroll
@@ -288,17 +356,34 @@ struct PositionKernel {
         }
 
         // ---- adjoint (mset.cu:232-271; STEP03_BACK.m:12-26) ----
-        for (int s = ns - 1; s >= 0; --s) {
+        for (int seg = nseg - 1; seg >= 0; --seg) {
+          const int s0 = ck ? seg * ck : 0, s1 = ck ? min(s0 + ck, ns) : ns;
+          if constexpr (MODE == kBatchCk) {
+            if (ck) {
+              // park the adjoint state, recompute the waves s0+1 .. s1 of the
+              // segment from its checkpoint, restore the state
+              sync_all();
+              for (int i = threadIdx.x; i < N * G::S; i += G::NT) park[i] = buf[i];
+              sync_all();
+              recompute(a, t, s0, s1, buf, tw, py, px, save + (size_t)seg * NN, recbuf);
+              sync_all();
+              for (int i = threadIdx.x; i < N * G::S; i += G::NT) buf[i] = park[i];
+              sync_all();
+            }
+          }
+          for (int s = s1 - 1; s >= s0; --s) {
             // REF: the wave saved after slab s (mset.cu:248-251); EXACT: the wave entering slab s
             const int ws = (METHOD == kSSET || ADJ == kEXACT) ? s : s + 1;
+            const float2 *wave = !ck ? save + (size_t)ws * NN
+                                     : (ws == s0 ? save + (size_t)seg * NN : recbuf + (size_t)(ws - s0 - 1) * NN);
             // the saved wave was written long ago (DRAM); have it in L2 by the row pass
-            prefetch_l2(save + (size_t)ws * NN, (unsigned)(sizeof(float2) * NN));
+            prefetch_l2(wave, (unsigned)(sizeof(float2) * NN));
             col_passA<G, +1, false>(buf, tw);
             sync_all();
             row_passB<G, +1>(buf);
             sync_rows();
             auto pf = [&](int y, int n1, TSPre<G> &pre) {
-                const float2 *sv = save + (size_t)ws * NN + (size_t)y * N + n1;
+                const float2 *sv = wave + (size_t)y * N + n1;
 #pragma unroll
                 for (int j = 0; j < R2; ++j) {
                     pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
@@ -347,6 +432,7 @@ struct PositionKernel {
                 row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop);
                 sync_all();
             }
+          }
         }
         // buf now holds chi0 (real space, natural order); save[0] holds psi0.
 
@@ -452,8 +538,7 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     // sit in front of every dependent load
     __shared__ TiltDev s_tilt;
     load_tables<G>(buf, a);
-    const int nsave = (METHOD == kSSET ? 1 : a.ns) + 1;
-    float2 *save = a.save + (size_t)blockIdx.x * nsave * G::N * G::N;
+    float2 *save = a.save + (size_t)blockIdx.x * a.slots * G::N * G::N;
     __syncthreads();
     using K = PositionKernel<G, METHOD, ADJ, MODE>;
     if constexpr (MODE == kSeq) {
@@ -576,6 +661,7 @@ int geo_positions(int method, int adjoint, int mode, const LaunchArgs &a, int gr
     MSET_L(kMSET, kREF, kSeq) MSET_L(kMSET, kREF, kBatch) MSET_L(kMSET, kEXACT, kSeq) MSET_L(kMSET, kEXACT, kBatch)
     MSET_L(kSSET, kREF, kSeq) MSET_L(kSSET, kREF, kBatch) MSET_L(kSSET, kEXACT, kSeq) MSET_L(kSSET, kEXACT, kBatch)
     MSET_L(kMSET, kREF, kErr) MSET_L(kSSET, kREF, kErr) MSET_L(kMSET, kREF, kSim) MSET_L(kSSET, kREF, kSim)
+    MSET_L(kMSET, kREF, kBatchCk) MSET_L(kMSET, kEXACT, kBatchCk)
 #undef MSET_L
     return (int)cudaErrorInvalidValue;
 }

@@ -203,6 +203,8 @@ extern "C" int mset_batch_gradient_noalloc(int device, void *stream, int n, int 
         a.ns = ns;
         a.sdz = sigma * potential_pixelsize;
         a.center = (float)std::round((n + 1.0f) / 2.0f);
+        a.ckpt = 0;
+        a.slots = ns + 1;  // one scratch slot of (ns + 1) waves per CTA, as sized above
         if ((rc = g->run(method, adjoint, a, grid, st)) != 0) break;
         k_noalloc_unscramble<<<64, 256, 0, st>>>(qacc, probe_out_dev, n, g->r1);
         e = cudaGetLastError();
