@@ -31,6 +31,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 
+# DRAM bytes per slice-propagation of k_positions at n = 128, 64 slabs,
+# measured with ncu on 128 positions (8192 units): (1.077490 + 1.111658) GB
+TRAFFIC_PER_UNIT = (1.077490e9 + 1.111658e9) / 8192
+
+
 def flops_per_unit(n: int) -> float:
     """FFTW convention: 4 FFTs of n x n (5 N^2 log2 N^2 each) + 32 N^2 pointwise."""
     n2 = n * n
@@ -198,6 +203,11 @@ def run_ours(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         it_ms = float(t.item())
 
+    # the plain form (reference semantics: one position after another, each
+    # updating volume, probe and position; mset_run) and the reference's own
+    # CUDA module (oracle/_ref, cuFFT) on a sample of the same tilt
+    plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (rank == 0 and not args.no_plain) else None
+
     # end to end through the C ABI with host buffers: volumes in, gradients out
     vols = [np.ascontiguousarray(0.5 * v) for v in spec.volumes]
     grad = np.zeros((cfg.n_tilts, ns, n, n))
@@ -244,7 +254,15 @@ def run_ours(args):
                        "units_per_step_per_gpu": units, "l2": "inputs larger than L2 (1.4 GB amplitudes)",
                        "parallelism": f"tilt replicas x{world}"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak, "traffic": None,
+                         "frac": achieved / fp32_peak,
+                         # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_positions launch on
+                         # the mid_s capture (128 positions: 1.0775 GB + 1.1117 GB), scaled by units
+                         "traffic": TRAFFIC_PER_UNIT * units,
+                         "traffic_note": "bytes per launch from the ncu capture of the same kernel on 128 positions "
+                                         "(profiles/k_positions_mid_s.md), scaled by slice-propagations; "
+                                         "algorithmic bytes per unit 16*n^2 (saved wave write + read) + "
+                                         "4*n^2/slabs (amplitudes)",
+                         "algorithmic_bytes": units * (16 * n * n + 4 * n * n / ns),
                          "peak_source": f"nominal FP32 CUDA-core peak 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz "
                                         "(MEASURED_PEAKS has no FP32 figure)",
                          "flop_per_unit": flops_per_unit(n), "flop_per_position": flops_per_position(n)},
@@ -257,6 +275,7 @@ def run_ours(args):
                         "batched forward+adjoint pass, 21 forward rotations of the gradient, update, positivity, "
                         f"TV-FISTA lambda 1e-3 x {args.tv_iter} iterations, probe and position updates",
                 "slice_propagations_per_s": world * units / (it_ms / 1e3)},
+            "plain_forms": plain,
             "gpu_launches": args.steps * bs._lib.mset_batch_launch_count(bs._h),
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -266,6 +285,47 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def reference_cuda(args, cfg, spec, meas, units_per_pos: int) -> dict:
+    """Sequential (reference-semantics) GPU forms on the first positions of
+    tilt 0: this library's plain fused kernel (mset_run, one CTA walking the
+    positions in order) and, when built, the reference's own CUDA module
+    (src/CUDA/mset.cu + cuFFT via oracle/_ref).  Both: CUDA-event free host
+    timing around a synchronous call, after one warm-up call."""
+    from mset_b200 import Session
+
+    k = args.plain_positions
+    n = cfg.window
+    v = 0.5 * spec.volumes[0]
+    sx, sy, me = spec.scan_x[:k], spec.scan_y[:k], meas[:k]
+    step = (1e-3, 1e-6, 1e-3)
+    out = {"positions": k, "slabs": units_per_pos,
+           "what": "run_mset over the first positions of tilt 0 (sequential per-position updates)"}
+    with Session() as s:
+        for rep in range(2):
+            s.upload(v, spec.probe, spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx, scan_x=sx, scan_y=sy,
+                     measured=me, step_size=step, slice_binning=cfg.slice_binning)
+            t0 = time.perf_counter()
+            s.run(1)
+            dt = time.perf_counter() - t0
+        out["plain_gpu"] = {"value": k * units_per_pos / dt, "unit": "slice-propagations/s", "seconds": dt}
+    try:
+        from oracle import refharness
+        if refharness.available():
+            for rep in range(2):
+                r = refharness.RefSession()
+                r.upload(v, spec.probe, spec.prop, sigma=spec.sigma, dz=cfg.dx, scan_x=sx, scan_y=sy, measured=me,
+                         step=step, binning=cfg.slice_binning)
+                t0 = time.perf_counter()
+                r.run(1)
+                dt = time.perf_counter() - t0
+            out["reference_cuda"] = {"value": k * units_per_pos / dt, "unit": "slice-propagations/s", "seconds": dt,
+                                     "what": "the reference's src/CUDA module (cuFFT, ~18*slabs+60 launches per "
+                                             "position), compiled unchanged for sm_100a"}
+    except Exception as e:  # the checker build is optional
+        out["reference_cuda"] = {"unavailable": str(e)[:200]}
+    return out
 
 
 def cpu_sample_positions(cores: int) -> int:
@@ -350,6 +410,8 @@ def main():
     ap.add_argument("--config", default="mid")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-iter", action="store_true", help="skip the full-iteration timing")
+    ap.add_argument("--no-plain", action="store_true", help="skip the sequential-form timings")
+    ap.add_argument("--plain-positions", type=int, default=32, help="positions in the sequential-form sample")
     ap.add_argument("--tv-iter", type=int, default=300, help="TV-FISTA inner iterations per iteration")
     args = ap.parse_args()
     if args.impl == "reference":
