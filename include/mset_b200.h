@@ -159,6 +159,13 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 
+/* storage of the measured patterns of a batched session: on != 0 keeps the
+ * counts as BF16 (2 bytes per pixel instead of 4; integers up to 256 are
+ * exact, larger counts are rounded to 8 significant bits) and takes the square
+ * root in FP32 when they are read; the loss accumulates in FP32 per pixel and
+ * FP64 per position.  Applies to measured patterns set after the call. */
+int mset_batch_set_amplitude_bf16(mset_session *s, int on);
+
 /* checkpointing of the batched pass: keep the wave entering every k-th slab
  * and recompute a segment's waves right before its adjoint (one extra forward
  * per slab, (ceil(ns/k) + k + 2) instead of (ns + 1) saved n x n waves per

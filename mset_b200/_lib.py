@@ -52,6 +52,7 @@ SIGNATURES = {
     "mset_batch_launch_count": (C.c_int, [C.c_void_p]),
     "mset_rotate_volume": (C.c_int, [C.c_void_p, _F, _F, C.c_int, _F, _F, _F, C.c_double, C.c_double, C.c_double,
                                      C.c_int]),
+    "mset_batch_set_amplitude_bf16": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_batch_set_checkpoint": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_batch_iteration_setup": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mset_batch_set_rec": (C.c_int, [C.c_void_p, _F]),

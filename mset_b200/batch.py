@@ -109,6 +109,10 @@ class BatchSession:
         check("mset_batch_time", self._lib.mset_batch_time(self._h, int(reps), dptr(ms)))
         return float(ms[0])
 
+    def set_amplitude_bf16(self, on: bool = True):
+        """keep measured counts as BF16 (set before the measured patterns)"""
+        check("mset_batch_set_amplitude_bf16", self._lib.mset_batch_set_amplitude_bf16(self._h, int(bool(on))))
+
     def set_checkpoint(self, k: int):
         """keep the wave entering every k-th slab and recompute the rest in the
         adjoint (0: keep all)"""

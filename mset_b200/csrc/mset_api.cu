@@ -77,6 +77,7 @@ struct TiltBufs {
     DevBuf<float> V;
     DevBuf<float2> Q;
     DevBuf<float> amp;
+    DevBuf<unsigned short> ampb;  // BF16 counts (batched sessions with BF16 storage)
     DevBuf<float> sx, sy;
     DevBuf<double> grad, qacc, posdir;
     int npos = 0;
@@ -110,6 +111,7 @@ struct mset_session {
     DevBuf<float> inten;
     int save_slots = 0;
     int ckpt = 0;  // checkpoint interval of the batched pass (0: keep every wave)
+    int amp_bf16 = 0;  // batched sessions: measured counts stored as BF16
     std::vector<TiltDev> h_tilts;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // batched iteration (rotate -> pass -> rotate back -> update -> TV)
@@ -246,11 +248,18 @@ int upload_tilt_probe(mset_session *s, TiltBufs &t, const float *probe) {
 int upload_tilt_measured(mset_session *s, TiltBufs &t, const float *meas) {
     const size_t n2 = (size_t)s->n * s->n;
     const size_t cnt = n2 * t.npos;
-    CK(t.amp.ensure(cnt));
     if (cnt == 0) return 0;
     CK(s->meas_tmp.ensure(std::max(s->meas_tmp.n, cnt)));
     CK(cudaMemcpyAsync(s->meas_tmp.p, meas, sizeof(float) * cnt, cudaMemcpyHostToDevice, s->st));
-    CKL(launch_prep_amp(s->plan, s->meas_tmp.p, t.amp.p, t.npos, s->st), "prep_amp");
+    if (s->batch && s->amp_bf16) {
+        t.amp.release();
+        CK(t.ampb.ensure(cnt));
+        CKL(launch_prep_amp_bf16(s->plan, s->meas_tmp.p, t.ampb.p, t.npos, s->st), "prep_amp_bf16");
+    } else {
+        t.ampb.release();
+        CK(t.amp.ensure(cnt));
+        CKL(launch_prep_amp(s->plan, s->meas_tmp.p, t.amp.p, t.npos, s->st), "prep_amp");
+    }
     return 0;
 }
 
@@ -263,6 +272,7 @@ int refresh_tilt_table(mset_session *s) {
         d.V = t.V.p;
         d.Q = t.Q.p;
         d.amp = t.amp.p;
+        d.ampb = t.ampb.p;
         d.sx = t.sx.p;
         d.sy = t.sy.p;
         d.grad = t.grad.p;
@@ -314,6 +324,10 @@ LaunchArgs base_args(mset_session *s) {
 
 int launch_queue(mset_session *s, int method, int adjoint, int mode) {
     if (mode == kBatch && method == kMSET && s->ckpt > 0 && s->ckpt < s->ns) mode = kBatchCk;
+    if (mode != kSim)
+        for (const TiltBufs &t : s->tilts)
+            if (t.npos > 0 && !t.amp.p && !t.ampb.p)
+                return fail(MSET_E_STATE, "measured patterns not set for every tilt");
     const int grid = persistent_grid(s, s->total_pos);
     int rc = ensure_save(s, grid);
     if (rc) return rc;
@@ -541,7 +555,6 @@ int mset_batch_setup(mset_session *s, const mset_batch_args *a) {
         CK(t.V.ensure(n2 * s->nz));
         CK(t.T.ensure(n2 * nsg));
         CK(t.Q.ensure(n2));
-        CK(t.amp.ensure(n2 * t.npos));
         CK(t.sx.ensure(std::max(1, t.npos)));
         CK(t.sy.ensure(std::max(1, t.npos)));
         CK(t.grad.ensure(n2 * nsg));
@@ -1104,6 +1117,13 @@ int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_iter = ms / niter;
+    return 0;
+}
+
+int mset_batch_set_amplitude_bf16(mset_session *s, int on) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    s->amp_bf16 = on ? 1 : 0;
     return 0;
 }
 

@@ -38,6 +38,9 @@ int launch_positions(const Plan &pl, int method, int adjoint, int mode, const La
 int launch_prep_amp(const Plan &pl, const float *meas, float *amp, long npos, cudaStream_t st) {
     return pl.ops->prep_amp(meas, amp, npos, st);
 }
+int launch_prep_amp_bf16(const Plan &pl, const float *meas, unsigned short *ib, long npos, cudaStream_t st) {
+    return pl.ops->prep_amp_bf16(meas, ib, npos, st);
+}
 int launch_prep_prop(const Plan &pl, const float *prop, float2 *pscr, cudaStream_t st) {
     return pl.ops->prep_prop(prop, pscr, st);
 }

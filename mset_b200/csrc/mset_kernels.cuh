@@ -30,6 +30,7 @@ struct TiltDev {
     double *err;         // [1] sum over positions and pixels of (A-M)^2
     float *inten;        // kSim: [npos][n][n] centred |Psi|^2
     const float2 *T;     // [ns][n][n] precomputed transmission slabs, or null (computed from V)
+    const unsigned short *ampb;  // [npos][n][n] scrambled ifftshift(I_meas) as BF16 bits, or null (use amp)
     int npos;
     int pad_;
 };
@@ -65,6 +66,7 @@ struct GeoOps {
     size_t smem;
     int (*positions)(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st);
     int (*prep_amp)(const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
+    int (*prep_amp_bf16)(const float *meas_centred, unsigned short *i_scr, long npos, cudaStream_t st);
     int (*prep_prop)(const float *prop_centred, float2 *pscr, cudaStream_t st);
     int (*probe_q)(bool to_q, const float2 *in, float2 *out, const float2 *twn, cudaStream_t st);
 };
@@ -80,6 +82,8 @@ bool plan_for(int n, Plan *p);
 int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,
                      cudaStream_t st);
 int launch_prep_amp(const Plan &pl, const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
+int launch_prep_amp_bf16(const Plan &pl, const float *meas_centred, unsigned short *i_scr, long npos,
+                         cudaStream_t st);
 int launch_prep_prop(const Plan &pl, const float *prop_centred, float2 *pscr, cudaStream_t st);
 int launch_probe_to_q(const Plan &pl, const float2 *probe, float2 *q, const float2 *twn, cudaStream_t st);
 int launch_q_to_probe(const Plan &pl, const float2 *q, float2 *probe, const float2 *twn, cudaStream_t st);

@@ -14,6 +14,7 @@
 // accumulates the gradients of every position of every tilt in FP64
 // (the batched method).  kErr is run_error_mset/_sset (mset.cu:557-810).
 #pragma once
+#include <cuda_bf16.h>
 #include "fft_core.cuh"
 #include "mset_kernels.cuh"
 
@@ -121,7 +122,12 @@ struct PositionKernel {
 
     // measured amplitude at scrambled location (Ly, Lx): prepared sqrt(I) in
     // scrambled layout, or (kBatchCentred) gathered from the centred pattern
-    static __device__ __forceinline__ float meas_amp(const float *amp, int Ly, int Lx) {
+    static __device__ __forceinline__ float meas_amp(const float *amp, const unsigned short *ampb, int Ly, int Lx) {
+        if (ampb) {
+            // measured counts stored as BF16 (exact for integers <= 256); sqrt in FP32
+            const unsigned short b = ampb[(size_t)Ly * N + Lx];
+            return sqrtf(__uint_as_float((unsigned)b << 16));
+        }
         if constexpr (MODE == kBatchCentred) {
             const int h = (N + 1) / 2;
             int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
@@ -306,7 +312,8 @@ struct PositionKernel {
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
         double err = 0.0;
-        const float *amp = t.amp + (size_t)p * NN;
+        const float *amp = t.amp ? t.amp + (size_t)p * NN : nullptr;
+        const unsigned short *ampb = t.ampb ? t.ampb + (size_t)p * NN : nullptr;
         if constexpr (MODE == kSim || MODE == kErr) {
             col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
@@ -321,7 +328,7 @@ struct PositionKernel {
                         t.inten[(size_t)p * NN + (size_t)r * N + c] = a2;
                     } else {
                         const float A = sqrtf(a2 + 1e-30f);
-                        const float M = meas_amp(amp, y0 + j, x);
+                        const float M = meas_amp(amp, ampb, y0 + j, x);
                         const float d = A - M;
                         err += (double)(d * d);
                     }
@@ -340,7 +347,7 @@ struct PositionKernel {
                 for (int j = 0; j < R1; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     const float A = sqrtf(a2 + 1e-30f);
-                    const float M = meas_amp(amp, y0 + j, x);
+                    const float M = meas_amp(amp, ampb, y0 + j, x);
                     const float d = A - M;
                     err += (double)(d * d);
                     float2 r = cscale(v[j], 1.0f - M / A);
@@ -584,6 +591,23 @@ __global__ void k_prep_amp(const float *meas, float *amp, long npos) {
 }
 
 template <class G>
+__global__ void k_prep_amp_bf16(const float *meas, unsigned short *ib, long npos) {
+    // ib[p][Ly][Lx] = bf16(ifftshift(I)[scr(Ly)][scr(Lx)]), round to nearest even
+    const long total = npos * (long)G::N * G::N;
+    const int h = (G::N + 1) / 2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long p = i / ((long)G::N * G::N);
+        const int l = (int)(i % ((long)G::N * G::N));
+        const int Ly = l / G::N, Lx = l % G::N;
+        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        if (r < 0) r += G::N;
+        if (c < 0) c += G::N;
+        const __nv_bfloat16 v = __float2bfloat16_rn(meas[p * G::N * G::N + (long)r * G::N + c]);
+        ib[i] = __bfloat16_as_ushort(v);
+    }
+}
+
+template <class G>
 __global__ void k_prep_prop(const float2 *prop, float2 *pscr) {
     // pscr[Ly][Lx] = ifftshift(prop)[scr(Ly)][scr(Lx)] / N^2  (mex_main.cu:80-83)
     const int h = (G::N + 1) / 2;
@@ -673,6 +697,12 @@ int geo_prep_amp(const float *meas, float *amp, long npos, cudaStream_t st) {
 }
 
 template <class G>
+int geo_prep_amp_bf16(const float *meas, unsigned short *ib, long npos, cudaStream_t st) {
+    k_prep_amp_bf16<G><<<1184, 256, 0, st>>>(meas, ib, npos);
+    return (int)cudaGetLastError();
+}
+
+template <class G>
 int geo_prep_prop(const float *prop, float2 *pscr, cudaStream_t st) {
     k_prep_prop<G><<<148, 256, 0, st>>>(reinterpret_cast<const float2 *>(prop), pscr);
     return (int)cudaGetLastError();
@@ -707,6 +737,7 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
                                     smem_bytes<Geo##N_>(),                             \
                                     &geo_positions<Geo##N_>,                           \
                                     &geo_prep_amp<Geo##N_>,                            \
+                                    &geo_prep_amp_bf16<Geo##N_>,                       \
                                     &geo_prep_prop<Geo##N_>,                           \
                                     &geo_probe_q<Geo##N_>};                            \
     }

@@ -164,3 +164,60 @@ def test_checkpointed_pass_matches_full_storage(gpu_available, k):
                                   dz=c["dz"], binning=1)
     assert rel_l2(outs[1]["grad"][0], g) < TOL
     assert rel_l2(np.fft.fft2(outs[1]["probe"][0]), pa) < TOL
+
+
+def _bf16_round(x):
+    """float32 -> nearest BF16 (ties to even), returned as float32"""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16 << 16
+    return b.astype(np.uint32).view(np.float32)
+
+
+def test_bf16_counts_integer_patterns_are_exact(gpu_available):
+    """integer counts <= 256 are exact in BF16: the BF16-stored pass gives the
+    FP32-stored pass's gradients (only the FP64 atomics' order differs)"""
+    c = small_case(n=64, nz=6, npos=5, b=2, seed=31, defocus=15.0, jitter=6.0, strength=STRENGTH)
+    scale = 250.0 / c["meas"].max()
+    meas = np.rint(c["meas"] * scale).astype(np.float32)
+    probe = c["probe"] * np.sqrt(scale)
+    outs = []
+    for bf in (False, True):
+        bs = BatchSession(n=64, nz=6, npos=[5], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"],
+                          slice_binning=2)
+        bs.set_amplitude_bf16(bf)
+        bs.set_tilt(0, probe=probe, scan_x=c["sx"], scan_y=c["sy"], measured=meas, volume=c["V"])
+        outs.append(bs.gradient())
+        bs.close()
+    for key in ("grad", "probe", "posdir", "err"):
+        assert rel_l2(outs[1][key], outs[0][key]) < 1e-9, key
+
+
+def test_bf16_counts_match_oracle_on_rounded_data(gpu_available):
+    """general counts: the BF16-stored pass equals the FP64 oracle run on the
+    BF16-rounded patterns (relative L2 <= 1e-4); the rounding itself is the
+    only difference from FP32 storage"""
+    c = small_case(n=128, nz=4, npos=3, b=2, seed=5, defocus=15.0, jitter=6.0, strength=STRENGTH)
+    meas = (c["meas"] * 3e3).astype(np.float32)
+    probe = c["probe"] * np.sqrt(3e3)
+    bs = BatchSession(n=128, nz=4, npos=[3], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"],
+                      slice_binning=2, adjoint=MSET_ADJOINT_EXACT)
+    bs.set_amplitude_bf16(True)
+    bs.set_tilt(0, probe=probe, scan_x=c["sx"], scan_y=c["sy"], measured=meas, volume=c["V"])
+    out = bs.gradient()
+    bs.close()
+    g, pa, pd, e = O.batched_tilt(c["V"], probe, c["prop"], c["sx"], c["sy"], _bf16_round(meas), sigma=c["sigma"],
+                                  dz=c["dz"], binning=2, adjoint=MSET_ADJOINT_EXACT)
+    assert rel_l2(out["grad"][0], g) < TOL
+    assert rel_l2(np.fft.fft2(out["probe"][0]), pa) < TOL
+    assert rel_l2(out["posdir"], pd) < 3e-4
+    assert abs(out["err"][0] - e) <= TOL * e
+
+
+def test_gradient_without_measured_patterns_is_an_error(gpu_available):
+    import mset_b200
+    c = small_case(n=24, nz=2, npos=2)
+    bs = BatchSession(n=24, nz=2, npos=[2], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+    bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], volume=c["V"])
+    with pytest.raises(mset_b200.MsetError, match="measured patterns"):
+        bs.gradient()
+    bs.close()
