@@ -207,6 +207,7 @@ def run_ours(args):
     # updating volume, probe and position; mset_run) and the reference's own
     # CUDA module (oracle/_ref, cuFFT) on a sample of the same tilt
     plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (rank == 0 and not args.no_plain) else None
+    uneven = uneven_batch(args, local) if (rank == 0 and args.uneven) else None
 
     # end to end through the C ABI with host buffers: volumes in, gradients out
     vols = [np.ascontiguousarray(0.5 * v) for v in spec.volumes]
@@ -276,6 +277,7 @@ def run_ours(args):
                         f"TV-FISTA lambda 1e-3 x {args.tv_iter} iterations, probe and position updates",
                 "slice_propagations_per_s": world * units / (it_ms / 1e3)},
             "plain_forms": plain,
+            "uneven_batch": uneven,
             "gpu_launches": args.steps * bs._lib.mset_batch_launch_count(bs._h),
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -328,6 +330,69 @@ def reference_cuda(args, cfg, spec, meas, units_per_pos: int) -> dict:
     return out
 
 
+def uneven_batch(args, device: int) -> dict:
+    """Six tilt series of uneven size (windows 64^2-160^2, 11-31 tilts, 32-96
+    slabs) as one group pass: every series' persistent kernel, with the batch
+    shape (persistent CTAs, checkpoint interval) and the schedule (serial or
+    concurrent with SMs split by work) picked by the library's autotuner, the
+    pass captured as one CUDA graph.  Beam-frame volumes are Fourier-shear
+    rotations of each series' lab-frame volume; intensities are simulated by
+    the library's forward model with seeded Poisson noise at each series' dose."""
+    import torch
+
+    from mset_b200 import Session, synth
+    from mset_b200.batch import BatchSession, SeriesGroup
+
+    t_setup = time.perf_counter()
+    members, rows = [], []
+    units = positions = 0
+    with Session(device) as rot:
+        for cfg in synth.UNEVEN:
+            spec = synth.make_specimen(cfg, per_tilt=False)
+            n, nv = cfg.window, cfg.vol[0]
+            ns = -(-nv // cfg.slice_binning)
+            npos = [spec.scan_x.size] * cfg.n_tilts
+            bs = BatchSession(n=n, nz=nv, npos=npos, prop=spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx,
+                              slice_binning=cfg.slice_binning, device=device)
+            vols = [synth.pad_lateral(rot.rotate_volume(spec.lab, a, inverse=True), n) for a in spec.angles]
+            for j, v in enumerate(vols):
+                bs.set_tilt(j, probe=spec.probe, scan_x=spec.scan_x, scan_y=spec.scan_y, volume=v)
+            inten = torch.from_numpy(bs.simulate()).to(f"cuda:{device}")
+            g = torch.Generator(device=f"cuda:{device}")
+            g.manual_seed(cfg.seed + 1000)
+            meas = torch.poisson(inten.clamp_min(0), generator=g).cpu().numpy()
+            del inten
+            off = 0
+            for j, v in enumerate(vols):
+                bs.set_tilt(j, measured=meas[off:off + npos[j]], volume=0.5 * v)
+                off += npos[j]
+            del meas
+            members.append(bs)
+            p = sum(npos)
+            units += p * ns
+            positions += p
+            rows.append({"series": cfg.name, "window": n, "volume_edge": nv, "slabs": ns, "tilts": cfg.n_tilts,
+                         "scan": list(cfg.scan), "positions": p, "dose": cfg.dose})
+    t_setup = time.perf_counter() - t_setup
+    grp = SeriesGroup(members, device=device)
+    ms_untuned = grp.time(max(1, min(args.steps, 2)), use_graph=True)
+    t0 = time.perf_counter()
+    sched = grp.tune(0.0)
+    t_tune = time.perf_counter() - t0
+    ms = grp.time(args.steps, use_graph=True)
+    for r, bs in zip(rows, members):
+        r["shape"] = {k: v for k, v in bs.shape().items() if k != "candidates"}
+    grp.close()
+    for bs in members:
+        bs.close()
+    return {"value": units / (ms / 1e3), "unit": "slice-propagations/s", "ms_per_pass": ms,
+            "units_per_pass": units, "positions": positions,
+            "schedule": "concurrent" if sched == 1 else "serial",
+            "untuned_serial_ms_per_pass": ms_untuned, "tune_s": t_tune, "setup_s": t_setup,
+            "series": rows,
+            "what": "6 tilt series of uneven size in one CUDA-graph group pass, shapes and schedule autotuned"}
+
+
 def cpu_sample_positions(cores: int) -> int:
     return int(max(8, min(96, 6 * cores)))
 
@@ -356,7 +421,6 @@ def run_reference(args):
         return
     from mset_b200 import synth
     from oracle import oracle as O
-    from tests.helpers import small_case  # noqa: F401
 
     cfg = synth.CONFIGS[args.config]
     spec = synth.make_specimen(cfg, with_volumes=False)
@@ -413,6 +477,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the sequential-form timings")
     ap.add_argument("--plain-positions", type=int, default=32, help="positions in the sequential-form sample")
     ap.add_argument("--tv-iter", type=int, default=300, help="TV-FISTA inner iterations per iteration")
+    ap.add_argument("--uneven", action="store_true", help="also time the uneven-size 6-series group pass")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

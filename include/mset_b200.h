@@ -172,6 +172,60 @@ int mset_batch_set_amplitude_bf16(mset_session *s, int on);
  * resident CTA); k = 0 or k >= ns keeps every wave */
 int mset_batch_set_checkpoint(mset_session *s, int k);
 
+/* results of the last batched pass (mset_batch_gradient's outputs, any NULL)
+ * without running a pass: for sessions run through a group */
+int mset_batch_read_gradient(mset_session *s, double *grad, double *probe, double *posdir, double *err);
+
+/* ---- autotuner ------------------------------------------------------------------
+ * Has no counterpart in the reference (its per-position launches have no batch
+ * shape).  Times the batched pass on a sample of the session's own positions
+ * (up to 4 x SMs x resident CTAs) for every shape whose saved-wave storage fits
+ * mem_budget_bytes (0: no limit) and keeps the fastest, or among shapes within
+ * 1% of it the one using less memory.  Shape = persistent CTAs (SMs x CTAs per
+ * SM, i.e. positions in flight) x checkpoint interval k in {0, 2, 4, 8, 16}
+ * (k < slabs; k = 0 keeps every wave).  The choice stays with the session
+ * (mset_batch_set_checkpoint overrides k).  MSET_E_NOMEM when no shape fits. */
+typedef struct {
+    int32_t grid;           /* persistent CTAs */
+    int32_t ctas_per_sm;
+    int32_t checkpoint;     /* k */
+    int32_t candidates;     /* shapes timed */
+    double us_per_position; /* measured device time per position at this shape */
+    double save_bytes;      /* saved-wave storage at this shape */
+} mset_tune_result;
+int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out);
+/* the shape the next batched pass uses (candidates = 0; us_per_position = 0
+ * when the session was not tuned) */
+int mset_batch_get_tune(mset_session *s, mset_tune_result *out);
+
+/* ---- groups: several tilt series of uneven size in one pass --------------------
+ * Has no counterpart in the reference.  A group holds batched sessions of any
+ * window sizes, slab counts, scan counts and tilt counts on one device; one
+ * group pass runs every member's gradient pass (the member's own persistent
+ * kernel over all its positions) and leaves the results on the device
+ * (mset_batch_read_gradient).  Schedules: SERIAL, the members' kernels one after
+ * another, each with all SMs; CONCURRENT, all members' kernels at once on
+ * forked streams with the SMs split in proportion to each member's work
+ * (mset_split_ctas), so that they finish together.  With use_graph the pass is
+ * captured once as one CUDA graph and replayed (re-captured when a member's
+ * buffers or shape change).  Sessions must outlive the group. */
+#define MSET_GROUP_SERIAL 0
+#define MSET_GROUP_CONCURRENT 1
+typedef struct mset_group mset_group;
+int mset_group_create(int device, mset_group **out);
+int mset_group_destroy(mset_group *g);
+int mset_group_add(mset_group *g, mset_session *s);
+int mset_group_set_schedule(mset_group *g, int schedule);
+/* tunes every member (the budget split in proportion to the members' full
+ * saved-wave storage), then times both schedules and keeps the faster */
+int mset_group_tune(mset_group *g, double mem_budget_bytes, int *schedule_out);
+int mset_group_gradient(mset_group *g, int use_graph);
+int mset_group_time(mset_group *g, int reps, int use_graph, double *ms_per_pass);
+/* SM split of the concurrent schedule: one SM per member plus the remaining
+ * SMs by largest remainder of work[i] / sum(work); grid_out[i] = SMs_i x
+ * ctas_per_sm[i].  Pure host function. */
+int mset_split_ctas(int count, const double *work, const int *ctas_per_sm, int sms, int *grid_out);
+
 /* ---- batched iteration ---------------------------------------------------------
  * One iteration of the batched method on a cubic lab-frame volume rec (nv^3,
  * nv == nz, nv <= n, lateral zero-padding to the window):

@@ -63,6 +63,17 @@ SIGNATURES = {
     "mset_batch_device_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
                                          C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "mset_tv": (C.c_int, [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D]),
+    "mset_batch_read_gradient": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "mset_batch_tune": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "mset_batch_get_tune": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mset_group_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "mset_group_destroy": (C.c_int, [C.c_void_p]),
+    "mset_group_add": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mset_group_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
+    "mset_group_tune": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
+    "mset_group_gradient": (C.c_int, [C.c_void_p, C.c_int]),
+    "mset_group_time": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D]),
+    "mset_split_ctas": (C.c_int, [C.c_int, _D, _I, C.c_int, _I]),
     "mset_batch_gradient_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_float, C.c_float, C.c_int] + [C.c_void_p] * 10),
 }
@@ -125,6 +136,26 @@ class IterArgs(C.Structure):
         ("tv_iter", C.c_int32),
         ("tv_fista", C.c_int32),
     ]
+
+
+class TuneResult(C.Structure):
+    """mset_tune_result (include/mset_b200.h)."""
+
+    _fields_ = [
+        ("grid", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("checkpoint", C.c_int32),
+        ("candidates", C.c_int32),
+        ("us_per_position", C.c_double),
+        ("save_bytes", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+MSET_GROUP_SERIAL = 0
+MSET_GROUP_CONCURRENT = 1
 
 
 class MsetError(RuntimeError):

@@ -64,12 +64,14 @@ class BatchSession:
             self._h, int(j), fptr(pr), fptr(sx), fptr(sy), fptr(me), fptr(vo)))
 
     def gradient(self, want=("grad", "probe", "posdir", "err")):
-        n2 = self.n * self.n
+        return self._fetch(self._lib.mset_batch_gradient, "mset_batch_gradient", want)
+
+    def _fetch(self, fn, name, want):
         g = np.zeros((self.ntilts, self.ns, self.n, self.n)) if "grad" in want else None
         p = np.zeros((self.ntilts, self.n, self.n, 2)) if "probe" in want else None
         d = np.zeros((int(self.npos.sum()), 2)) if "posdir" in want else None
         e = np.zeros(self.ntilts) if "err" in want else None
-        check("mset_batch_gradient", self._lib.mset_batch_gradient(self._h, dptr(g), dptr(p), dptr(d), dptr(e)))
+        check(name, fn(self._h, dptr(g), dptr(p), dptr(d), dptr(e)))
         out = {}
         if g is not None:
             out["grad"] = g
@@ -79,8 +81,23 @@ class BatchSession:
             out["posdir"] = d
         if e is not None:
             out["err"] = e
-        del n2
         return out
+
+    def read_gradient(self, want=("grad", "probe", "posdir", "err")):
+        """results of the last pass (e.g. one run through a SeriesGroup)"""
+        return self._fetch(self._lib.mset_batch_read_gradient, "mset_batch_read_gradient", want)
+
+    def tune(self, mem_budget_bytes: float = 0.0) -> dict:
+        """pick persistent CTAs and checkpoint interval by timing (include/mset_b200.h)"""
+        r = _lib.TuneResult()
+        check("mset_batch_tune", self._lib.mset_batch_tune(self._h, float(mem_budget_bytes), C.byref(r)))
+        return r.as_dict()
+
+    def shape(self) -> dict:
+        """the batch shape the next pass uses (mset_batch_get_tune)"""
+        r = _lib.TuneResult()
+        check("mset_batch_get_tune", self._lib.mset_batch_get_tune(self._h, C.byref(r)))
+        return r.as_dict()
 
     def error(self) -> np.ndarray:
         e = np.zeros(self.ntilts)
@@ -154,3 +171,55 @@ class BatchSession:
         ms = np.zeros(1)
         check("mset_batch_iterate_time", self._lib.mset_batch_iterate_time(self._h, int(niter), dptr(ms)))
         return float(ms[0])
+
+
+class SeriesGroup:
+    """Several batched sessions (tilt series of any window, slab, scan and
+    tilt counts) run as one pass (``mset_group_*`` in include/mset_b200.h)."""
+
+    def __init__(self, sessions: Sequence[BatchSession], device: int = 0):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        check("mset_group_create", self._lib.mset_group_create(int(device), C.byref(h)))
+        self._h = h
+        self.sessions = list(sessions)  # kept alive: the group borrows them
+        for s in self.sessions:
+            check("mset_group_add", self._lib.mset_group_add(self._h, s._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mset_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_schedule(self, schedule: int):
+        check("mset_group_set_schedule", self._lib.mset_group_set_schedule(self._h, int(schedule)))
+
+    def tune(self, mem_budget_bytes: float = 0.0) -> int:
+        sched = C.c_int()
+        check("mset_group_tune", self._lib.mset_group_tune(self._h, float(mem_budget_bytes), C.byref(sched)))
+        return int(sched.value)
+
+    def run(self, use_graph: bool = True):
+        check("mset_group_gradient", self._lib.mset_group_gradient(self._h, int(bool(use_graph))))
+
+    def time(self, reps: int, use_graph: bool = True) -> float:
+        ms = np.zeros(1)
+        check("mset_group_time", self._lib.mset_group_time(self._h, int(reps), int(bool(use_graph)), dptr(ms)))
+        return float(ms[0])
+
+
+def split_ctas(work, ctas_per_sm, sms: int) -> np.ndarray:
+    """mset_split_ctas: CTAs per member of a concurrent group pass"""
+    lib = _lib.load()
+    w = np.ascontiguousarray(np.asarray(work, dtype=np.float64))
+    o = np.ascontiguousarray(np.asarray(ctas_per_sm, dtype=np.int32))
+    out = np.zeros(w.size, np.int32)
+    check("mset_split_ctas", lib.mset_split_ctas(int(w.size), dptr(w), o.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 int(sms), out.ctypes.data_as(C.POINTER(C.c_int32))))
+    return out

@@ -112,6 +112,8 @@ struct mset_session {
     int save_slots = 0;
     int ckpt = 0;  // checkpoint interval of the batched pass (0: keep every wave)
     int amp_bf16 = 0;  // batched sessions: measured counts stored as BF16
+    int tuned_grid = 0;  // CTAs of the batched pass picked by the tuner (0: every resident CTA)
+    double tuned_us_per_pos = 0;  // tuner's measured cost of one position at tuned_grid
     std::vector<TiltDev> h_tilts;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // batched iteration (rotate -> pass -> rotate back -> update -> TV)
@@ -289,6 +291,7 @@ int refresh_tilt_table(mset_session *s) {
 }
 
 int persistent_grid(mset_session *s, int items) {
+    if (s->tuned_grid > 0) return std::max(1, std::min(s->tuned_grid, items));
     // CTAs resident per SM for this kernel's shared memory and threads
     const size_t per_sm_smem = 227 * 1024;
     int by_smem = (int)(per_sm_smem / (s->plan.smem + 1024));
@@ -322,21 +325,37 @@ LaunchArgs base_args(mset_session *s) {
     return a;
 }
 
-int launch_queue(mset_session *s, int method, int adjoint, int mode) {
-    if (mode == kBatch && method == kMSET && s->ckpt > 0 && s->ckpt < s->ns) mode = kBatchCk;
+int effective_mode(const mset_session *s, int method, int mode) {
+    return (mode == kBatch && method == kMSET && s->ckpt > 0 && s->ckpt < s->ns) ? kBatchCk : mode;
+}
+
+// host-side preparation of a queue launch with `grid` CTAs (not capturable:
+// allocation and a pageable copy of the tilt table)
+int queue_prepare(mset_session *s, int mode, int grid) {
     if (mode != kSim)
         for (const TiltBufs &t : s->tilts)
             if (t.npos > 0 && !t.amp.p && !t.ampb.p)
                 return fail(MSET_E_STATE, "measured patterns not set for every tilt");
-    const int grid = persistent_grid(s, s->total_pos);
     int rc = ensure_save(s, grid);
     if (rc) return rc;
-    rc = refresh_tilt_table(s);
-    if (rc) return rc;
+    return refresh_tilt_table(s);
+}
+
+// capturable part: reset the work counter and launch over the first nitems items
+int queue_enqueue(mset_session *s, int method, int adjoint, int mode, int grid, int nitems) {
     CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
     LaunchArgs a = base_args(s);
-    CKL(launch_positions(s->plan, method, adjoint, mode, a, grid, s->st), "position kernel launch");
+    a.nitems = nitems;
+    CKL(launch_positions(s->plan, method, adjoint, effective_mode(s, method, mode), a, grid, s->st),
+        "position kernel launch");
     return 0;
+}
+
+int launch_queue(mset_session *s, int method, int adjoint, int mode) {
+    const int grid = persistent_grid(s, s->total_pos);
+    int rc = queue_prepare(s, mode, grid);
+    if (rc) return rc;
+    return queue_enqueue(s, method, adjoint, mode, grid, s->total_pos);
 }
 
 int check_mode(int mode) {
@@ -626,14 +645,18 @@ static int batch_zero(mset_session *s) {
 }
 
 // transmission slabs of every tilt from the current volumes
-static int batch_transmission(mset_session *s) {
-    int rc = refresh_tilt_table(s);
-    if (rc) return rc;
+static int batch_transmission_enqueue(mset_session *s) {
     const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
     const int b = s->method == MSET_MODE_SSET ? s->nz : s->b;
     CKL(launch_transmission(s->d_tilts.p, (int)s->tilts.size(), s->n, s->nz, b, nsg, s->sigma * s->dz, s->st),
         "transmission");
     return 0;
+}
+
+static int batch_transmission(mset_session *s) {
+    int rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    return batch_transmission_enqueue(s);
 }
 
 static int batch_pass(mset_session *s) {
@@ -649,6 +672,13 @@ int mset_batch_gradient(mset_session *s, double *grad_out, double *probe_out, do
     int rc = batch_ok(s);
     if (rc) return rc;
     rc = batch_pass(s);
+    if (rc) return rc;
+    return mset_batch_read_gradient(s, grad_out, probe_out, posdir_out, err_out);
+}
+
+int mset_batch_read_gradient(mset_session *s, double *grad_out, double *probe_out, double *posdir_out,
+                             double *err_out) {
+    int rc = batch_ok(s);
     if (rc) return rc;
     const size_t n2 = (size_t)s->n * s->n;
     const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
@@ -1140,6 +1170,419 @@ int mset_batch_set_checkpoint(mset_session *s, int k) {
 int mset_batch_launch_count(mset_session *s) {
     if (!s) return fail(MSET_E_ARG, "null session");
     return 2;  // transmission slabs + position kernel
+}
+
+}  // extern "C"
+
+// ---- autotuner ----------------------------------------------------------------
+// The batched pass has two shape parameters that trade memory for speed: the
+// number of persistent CTAs (positions in flight; each owns a saved-wave slot
+// set) and the checkpoint interval k (slots per CTA: ns + 1 at k = 0,
+// ceil(ns/k) + k + 2 otherwise, with the forward of each segment recomputed in
+// the adjoint).  The tuner times every (CTAs per SM, k) pair whose saved-wave
+// storage fits the memory budget on a sample of the session's own positions
+// and keeps the fastest; among shapes within 1% of it, the one using less
+// memory.
+namespace {
+
+int occupancy_limit(const mset_session *s) {
+    const int by_smem = (int)((227 * 1024) / (s->plan.smem + 1024));
+    const int by_thr = 2048 / s->plan.nt;
+    return std::max(1, std::min(by_smem, by_thr));
+}
+
+double save_bytes(const mset_session *s, int grid, int k) {
+    return (double)grid * save_slots(s->ns, k) * s->n * s->n * sizeof(float2);
+}
+
+// one warm launch, then `reps` timed launches over the first nitems positions
+int time_queue(mset_session *s, int grid, int nitems, int reps, double *ms) {
+    int rc = queue_prepare(s, kBatch, grid);
+    if (rc) return rc;
+    rc = queue_enqueue(s, s->method, s->adjoint, kBatch, grid, nitems);
+    if (rc) return rc;
+    CK(cudaEventRecord(s->ev0, s->st));
+    for (int r = 0; r < reps; ++r) {
+        rc = queue_enqueue(s, s->method, s->adjoint, kBatch, grid, nitems);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(s->ev1, s->st));
+    CK(cudaEventSynchronize(s->ev1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, s->ev0, s->ev1));
+    *ms = t / reps;
+    return 0;
+}
+
+int tune_session(mset_session *s, double budget, mset_tune_result *out) {
+    const int occ = occupancy_limit(s);
+    std::vector<int> ks{0};
+    if (s->method == MSET_MODE_MSET)
+        for (int k : {2, 4, 8, 16})
+            if (k < s->ns) ks.push_back(k);
+    const int k_in = s->ckpt;
+    const int sample = std::min(s->total_pos, 4 * s->sms * occ);
+    int rc = batch_zero(s);
+    if (!rc) rc = batch_transmission(s);
+    if (rc) return rc;
+    int best_grid = 0, best_k = 0, timed = 0, last_grid = 0;
+    double best_us = 0, best_bytes = 0;
+    for (int c = 1; c <= occ; ++c) {
+        const int grid = std::max(1, std::min(s->sms * c, s->total_pos));
+        if (grid == last_grid) break;
+        last_grid = grid;
+        for (int k : ks) {
+            const double bytes = save_bytes(s, grid, k);
+            if (budget > 0 && bytes > budget) continue;
+            s->ckpt = k;
+            double ms = 0;
+            rc = time_queue(s, grid, sample, 2, &ms);
+            if (rc) {
+                s->ckpt = k_in;
+                return rc;
+            }
+            ++timed;
+            const double us = ms * 1e3 / sample;
+            const bool faster = !best_grid || us < 0.99 * best_us;
+            const bool tie_smaller = best_grid && us <= 1.01 * best_us && bytes < best_bytes;
+            if (faster || tie_smaller) {
+                if (faster || us < best_us) best_us = us;
+                best_grid = grid;
+                best_k = k;
+                best_bytes = bytes;
+            }
+        }
+    }
+    if (!best_grid) {
+        s->ckpt = k_in;
+        return fail(MSET_E_NOMEM, "no batch shape of the %d^2 window fits the memory budget of %.0f bytes", s->n,
+                    budget);
+    }
+    s->ckpt = best_k;
+    s->tuned_grid = best_grid;
+    s->tuned_us_per_pos = best_us;
+    s->grid_cache = 0;
+    drop_graph(s);
+    s->save.release();
+    rc = ensure_save(s, best_grid);
+    if (rc) return rc;
+    rc = batch_zero(s);  // the sample passes left partial sums
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    if (out) {
+        out->grid = best_grid;
+        out->ctas_per_sm = (best_grid + s->sms - 1) / s->sms;
+        out->checkpoint = best_k;
+        out->candidates = timed;
+        out->us_per_position = best_us;
+        out->save_bytes = best_bytes;
+    }
+    return 0;
+}
+
+}  // namespace
+
+// ---- groups of batched sessions -------------------------------------------------
+struct mset_group {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<mset_session *> m;
+    std::vector<cudaEvent_t> done;
+    int schedule = MSET_GROUP_SERIAL;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void *> sig;  // pointers and shapes the captured graph was built on
+};
+
+namespace {
+
+void group_drop_graph(mset_group *g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->exec = nullptr;
+    g->graph = nullptr;
+    g->sig.clear();
+}
+
+// work of a member in SM-time units: the tuner's measured cost, else a model
+// proportional to slabs x n^2 log2 n per position
+double member_work(const mset_session *s) {
+    if (s->tuned_us_per_pos > 0) return s->total_pos * s->tuned_us_per_pos;
+    return (double)s->total_pos * s->ns * s->n * s->n * std::log2((double)s->n) * 1e-6;
+}
+
+int group_grids(mset_group *g, std::vector<int> &grids) {
+    const int M = (int)g->m.size();
+    grids.assign(M, 0);
+    if (g->schedule == MSET_GROUP_SERIAL) {
+        for (int i = 0; i < M; ++i) grids[i] = persistent_grid(g->m[i], std::max(1, g->m[i]->total_pos));
+        return 0;
+    }
+    std::vector<double> w(M);
+    std::vector<int> occ(M);
+    for (int i = 0; i < M; ++i) {
+        mset_session *s = g->m[i];
+        w[i] = member_work(s);
+        occ[i] = s->tuned_grid > 0 ? std::max(1, (s->tuned_grid + s->sms - 1) / s->sms) : occupancy_limit(s);
+    }
+    int rc = mset_split_ctas(M, w.data(), occ.data(), g->m[0]->sms, grids.data());
+    if (rc) return rc;
+    for (int i = 0; i < M; ++i) grids[i] = std::max(1, std::min(grids[i], std::max(1, g->m[i]->total_pos)));
+    return 0;
+}
+
+// the capturable part of one group pass on g->st
+int group_enqueue(mset_group *g, const std::vector<int> &grids) {
+    CK(cudaEventRecord(g->fork, g->st));
+    const int M = (int)g->m.size();
+    for (int i = 0; i < M; ++i) {
+        mset_session *s = g->m[i];
+        const bool after_prev = g->schedule == MSET_GROUP_SERIAL && i > 0;
+        CK(cudaStreamWaitEvent(s->st, after_prev ? g->done[i - 1] : g->fork, 0));
+        int rc = batch_zero(s);
+        if (rc) return rc;
+        if (s->total_pos) {
+            rc = batch_transmission_enqueue(s);
+            if (!rc) rc = queue_enqueue(s, s->method, s->adjoint, kBatch, grids[i], s->total_pos);
+            if (rc) return rc;
+        }
+        CK(cudaEventRecord(g->done[i], s->st));
+    }
+    for (int i = 0; i < M; ++i) CK(cudaStreamWaitEvent(g->st, g->done[i], 0));
+    return 0;
+}
+
+int group_prepare(mset_group *g, std::vector<int> &grids) {
+    if (g->m.empty()) return fail(MSET_E_STATE, "empty group");
+    CK(cudaSetDevice(g->device));
+    int rc = group_grids(g, grids);
+    if (rc) return rc;
+    std::vector<const void *> sig;
+    sig.push_back(reinterpret_cast<const void *>((intptr_t)g->schedule));
+    for (size_t i = 0; i < g->m.size(); ++i) {
+        mset_session *s = g->m[i];
+        rc = queue_prepare(s, kBatch, grids[i]);
+        if (rc) return rc;
+        for (const void *p : {(const void *)s->d_tilts.p, (const void *)s->save.p, (const void *)s->items.p,
+                              (const void *)s->counter.p, (const void *)s->err.p})
+            sig.push_back(p);
+        sig.push_back(reinterpret_cast<const void *>((intptr_t)grids[i]));
+        sig.push_back(reinterpret_cast<const void *>((intptr_t)s->ckpt));
+        sig.push_back(reinterpret_cast<const void *>((intptr_t)s->total_pos));
+        for (const TiltBufs &t : s->tilts) {
+            sig.push_back(t.grad.p);
+            sig.push_back(t.qacc.p);
+        }
+    }
+    if (sig != g->sig) group_drop_graph(g);
+    g->sig.swap(sig);
+    return 0;
+}
+
+int group_launch(mset_group *g, const std::vector<int> &grids, bool use_graph) {
+    if (!use_graph) return group_enqueue(g, grids);
+    if (!g->exec) {
+        CK(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeRelaxed));
+        int rc = group_enqueue(g, grids);
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(g->st, &gr);
+        if (rc) {
+            if (gr) cudaGraphDestroy(gr);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "capturing the group pass");
+        g->graph = gr;
+        e = cudaGraphInstantiate(&g->exec, gr, 0);
+        if (e != cudaSuccess) {
+            group_drop_graph(g);
+            return cuda_fail(e, "instantiating the group pass");
+        }
+    }
+    CK(cudaGraphLaunch(g->exec, g->st));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (mem_budget_bytes < 0) return fail(MSET_E_ARG, "negative memory budget");
+    if (s->total_pos == 0) return fail(MSET_E_STATE, "no positions to tune on");
+    return tune_session(s, mem_budget_bytes, out);
+}
+
+int mset_batch_get_tune(mset_session *s, mset_tune_result *out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!out) return fail(MSET_E_ARG, "null output");
+    const int grid = persistent_grid(s, std::max(1, s->total_pos));
+    out->grid = grid;
+    out->ctas_per_sm = (grid + s->sms - 1) / s->sms;
+    out->checkpoint = s->ckpt;
+    out->candidates = 0;
+    out->us_per_position = s->tuned_us_per_pos;
+    out->save_bytes = save_bytes(s, grid, s->ckpt);
+    return 0;
+}
+
+int mset_split_ctas(int count, const double *work, const int *ctas_per_sm, int sms, int *grid_out) {
+    if (count <= 0 || !work || !ctas_per_sm || !grid_out || sms <= 0) return fail(MSET_E_ARG, "bad arguments");
+    if (count > sms) return fail(MSET_E_ARG, "more members (%d) than SMs (%d)", count, sms);
+    double tot = 0;
+    for (int i = 0; i < count; ++i) {
+        if (!(work[i] >= 0) || ctas_per_sm[i] <= 0) return fail(MSET_E_ARG, "bad work or occupancy of member %d", i);
+        tot += work[i];
+    }
+    // one SM each, the rest by largest remainder of the work share
+    std::vector<int> sm(count, 1);
+    const int spare = sms - count;
+    std::vector<std::pair<double, int>> rem;
+    int given = 0;
+    for (int i = 0; i < count; ++i) {
+        const double share = tot > 0 ? spare * work[i] / tot : (double)spare / count;
+        const int whole = (int)std::floor(share);
+        sm[i] += whole;
+        given += whole;
+        rem.push_back({share - whole, i});
+    }
+    std::stable_sort(rem.begin(), rem.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+        return a.first > b.first;
+    });
+    for (int r = 0; r < spare - given; ++r) sm[rem[r].second] += 1;
+    for (int i = 0; i < count; ++i) grid_out[i] = sm[i] * ctas_per_sm[i];
+    return 0;
+}
+
+int mset_group_create(int device, mset_group **out) {
+    if (!out) return fail(MSET_E_ARG, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) return fail(MSET_E_ARG, "device %d out of range", device);
+    mset_group *g = new mset_group;
+    g->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&g->ev1);
+    if (e != cudaSuccess) {
+        mset_group_destroy(g);
+        return cuda_fail(e, "group setup");
+    }
+    *out = g;
+    return 0;
+}
+
+int mset_group_destroy(mset_group *g) {
+    if (!g) return 0;
+    cudaSetDevice(g->device);
+    if (g->st) cudaStreamSynchronize(g->st);
+    group_drop_graph(g);
+    for (cudaEvent_t e : g->done) cudaEventDestroy(e);
+    if (g->fork) cudaEventDestroy(g->fork);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->st) cudaStreamDestroy(g->st);
+    delete g;
+    return 0;
+}
+
+int mset_group_add(mset_group *g, mset_session *s) {
+    if (!g) return fail(MSET_E_ARG, "null group");
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (s->device != g->device) return fail(MSET_E_ARG, "session on device %d, group on %d", s->device, g->device);
+    for (mset_session *o : g->m)
+        if (o == s) return fail(MSET_E_ARG, "session already in the group");
+    CK(cudaSetDevice(g->device));
+    cudaEvent_t e = nullptr;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    g->m.push_back(s);
+    g->done.push_back(e);
+    group_drop_graph(g);
+    return 0;
+}
+
+int mset_group_set_schedule(mset_group *g, int schedule) {
+    if (!g) return fail(MSET_E_ARG, "null group");
+    if (schedule != MSET_GROUP_SERIAL && schedule != MSET_GROUP_CONCURRENT)
+        return fail(MSET_E_ARG, "unknown schedule %d", schedule);
+    if (schedule != g->schedule) group_drop_graph(g);
+    g->schedule = schedule;
+    return 0;
+}
+
+int mset_group_gradient(mset_group *g, int use_graph) {
+    if (!g) return fail(MSET_E_ARG, "null group");
+    std::vector<int> grids;
+    int rc = group_prepare(g, grids);
+    if (rc) return rc;
+    rc = group_launch(g, grids, use_graph != 0);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(g->st));
+    return 0;
+}
+
+int mset_group_time(mset_group *g, int reps, int use_graph, double *ms_per_pass) {
+    if (!g || reps <= 0 || !ms_per_pass) return fail(MSET_E_ARG, "bad arguments");
+    std::vector<int> grids;
+    int rc = group_prepare(g, grids);
+    if (rc) return rc;
+    rc = group_launch(g, grids, use_graph != 0);  // warm (and capture)
+    if (rc) return rc;
+    CK(cudaEventRecord(g->ev0, g->st));
+    for (int r = 0; r < reps; ++r) {
+        rc = group_launch(g, grids, use_graph != 0);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(g->ev1, g->st));
+    CK(cudaEventSynchronize(g->ev1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, g->ev0, g->ev1));
+    *ms_per_pass = t / reps;
+    return 0;
+}
+
+int mset_group_tune(mset_group *g, double mem_budget_bytes, int *schedule_out) {
+    if (!g) return fail(MSET_E_ARG, "null group");
+    if (g->m.empty()) return fail(MSET_E_STATE, "empty group");
+    if (mem_budget_bytes < 0) return fail(MSET_E_ARG, "negative memory budget");
+    // the budget is split in proportion to each member's full-storage need
+    double need = 0;
+    for (mset_session *s : g->m) need += save_bytes(s, persistent_grid(s, std::max(1, s->total_pos)), 0);
+    for (mset_session *s : g->m) {
+        if (s->total_pos == 0) continue;
+        const double own = save_bytes(s, persistent_grid(s, std::max(1, s->total_pos)), 0);
+        const double b = mem_budget_bytes > 0 ? mem_budget_bytes * own / std::max(need, 1.0) : 0;
+        CK(cudaSetDevice(s->device));
+        s->tuned_grid = 0;
+        int rc = tune_session(s, b, nullptr);
+        if (rc) return rc;
+    }
+    // both schedules, timed on full passes
+    double best = 0;
+    int best_sched = MSET_GROUP_SERIAL;
+    for (int sched : {MSET_GROUP_SERIAL, MSET_GROUP_CONCURRENT}) {
+        int rc = mset_group_set_schedule(g, sched);
+        if (rc) return rc;
+        double ms = 0;
+        rc = mset_group_time(g, 2, 0, &ms);
+        if (rc) return rc;
+        if (sched == MSET_GROUP_SERIAL || ms < best) {
+            best = ms;
+            best_sched = sched;
+        }
+    }
+    int rc = mset_group_set_schedule(g, best_sched);
+    if (rc) return rc;
+    if (schedule_out) *schedule_out = best_sched;
+    return 0;
 }
 
 }  // extern "C"

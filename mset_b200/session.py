@@ -65,6 +65,23 @@ class Session:
     def __exit__(self, *exc):
         self.close()
 
+    # ---- volume operations of the reconstruction loop ----
+    def rotate_volume(self, vol, angles, *, inverse: bool = False, vec1=(0, 0, 1), vec2=(0, 1, 0),
+                      vec3=(1, 0, 0)) -> np.ndarray:
+        """Func_rot_3Dvol_FourierShear / Func_inv_rot_3Dvol_FourierShear of a
+        cubic [n][n][n] volume by (phi, theta, psi) degrees (mset_rotate_volume)"""
+        v = _c32(vol)
+        n = v.shape[0]
+        if v.shape != (n, n, n):
+            raise ValueError(f"cubic volume expected, got {v.shape}")
+        out = np.empty_like(v)
+        vecs = [np.ascontiguousarray(np.asarray(x, np.float32)) for x in (vec1, vec2, vec3)]
+        a = [float(x) for x in angles]
+        check("mset_rotate_volume", self._lib.mset_rotate_volume(self._h, fptr(v), fptr(out), n, fptr(vecs[0]),
+                                                                 fptr(vecs[1]), fptr(vecs[2]), a[0], a[1], a[2],
+                                                                 int(bool(inverse))))
+        return out
+
     # ---- 'upload' (mex_main.cu:42-95) ----
     def upload(self, rvol, probe, prop, *, sigma: float, potential_pixelsize: float,
                scan_x, scan_y, measured, step_size=(0.0, 0.0, 0.0), slice_binning: int = 1,

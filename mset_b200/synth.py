@@ -59,6 +59,18 @@ CONFIGS = {
                    defocus_A=50.0, C30_A=1e7, jitter_px=0.5),
 }
 
+# uneven-size batch: 6 independent tilt series run as one pass, windows 64^2 to
+# 160^2, scans 16x16 to 40x40, 11 to 31 tilts, 32 to 96 slabs, volume edges 64
+# to 128 voxels, doses 1e3 to 1e5 e-/probe
+UNEVEN = [
+    Config("uneven_64a", (64, 64, 64), 0.3, 64, (16, 16), 2.0, 11, 50.0, 2, 1e3, seed=101),
+    Config("uneven_96a", (96, 96, 96), 0.3, 96, (24, 24), 2.0, 15, 60.0, 2, 1e4, seed=102),
+    Config("uneven_128", (128, 128, 128), 0.3, 128, (32, 32), 3.0, 21, 60.0, 2, 1e5, seed=103),
+    Config("uneven_160", (96, 96, 96), 0.3, 160, (24, 24), 4.0, 31, 70.0, 1, 3e4, seed=104),
+    Config("uneven_64b", (64, 64, 64), 0.3, 64, (40, 40), 1.0, 31, 70.0, 2, 3e3, seed=105),
+    Config("uneven_96b", (96, 96, 96), 0.3, 96, (20, 20), 3.0, 11, 40.0, 1, 1e5, seed=106),
+]
+
 
 def tilt_angles(cfg: Config) -> np.ndarray:
     """[n_tilts, 3] (phi, theta, psi) in degrees; rotation about y only."""
@@ -159,7 +171,8 @@ class Specimen:
     natoms: int
 
 
-def make_specimen(cfg: Config, with_volumes: bool = True) -> Specimen:
+def make_specimen(cfg: Config, with_volumes: bool = True, per_tilt: bool = True) -> Specimen:
+    """per_tilt=False: only the lab-frame volume (tilts left to a rotation)"""
     rng = np.random.default_rng(cfg.seed)
     lam = physics.electron_wavelength(cfg.E0_kV * 1e3)
     sigma = physics.interaction_constant(cfg.E0_kV * 1e3)
@@ -169,7 +182,7 @@ def make_specimen(cfg: Config, with_volumes: bool = True) -> Specimen:
     lab = None
     if with_volumes:
         lab = voxelise(pos, peak, cfg.vol, cfg.dx, cfg.blob_sigma).astype(np.float32)
-        for th in angles[:, 1]:
+        for th in (angles[:, 1] if per_tilt else []):
             # beam frame of tilt th: the reference's Func_inv_rot_3Dvol_FourierShear
             # with (phi, theta, psi) = (0, th, 0) maps (x, 0, 0) to (x cos th, 0, x sin th)
             R = rot_y(-th)
