@@ -25,6 +25,10 @@
  *                the fastest (MATLAB dim-1) axis.
  * All pointers in this header are HOST pointers unless a name ends in _dev.
  *
+ * Window sizes n with compiled kernels: 24, 32, 48, 64, 96, 128, 160 (one CTA
+ * per probe position) and 256 (one position per cluster of 4 CTAs, the field
+ * split by rows over their shared memories).
+ *
  * Every function returns 0 on success or a negative MSET_E* status; it never
  * aborts.  mset_last_error() gives the message of the calling thread's last
  * failure.  A session is not thread-safe; different sessions are independent.

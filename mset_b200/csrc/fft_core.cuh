@@ -24,6 +24,7 @@
 // so one propagation slab costs six shared-memory round trips, with a
 // CTA-wide barrier only where row passes meet column passes.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -251,11 +252,40 @@ struct Geo {
     static constexpr int S = N + N / R1;  // padded row stride (elements)
     static constexpr int NRA = N * R1;    // row/col pass-A tasks (R2 points each)
     static constexpr int NRB = N * R2;    // row/col pass-B tasks (R1 points each)
+    static constexpr int CL = 1;          // CTAs sharing one field (thread-block cluster)
+    static constexpr int ROWS = N;        // rows of the field held by one CTA
+    static constexpr int FIELD = ROWS * S;
     static_assert(R1 * R2 == N, "N must equal R1*R2");
     __device__ __forceinline__ static int px(int x) { return x + x / R1; }
     __device__ __forceinline__ static int at(int y, int x) { return y * S + px(x); }
     // scrambled location -> frequency index
     __host__ __device__ __forceinline__ static int scr(int L) { return L / R1 + R2 * (L % R1); }
+    __device__ __forceinline__ static int rank() { return 0; }
+    __device__ __forceinline__ static int row0() { return 0; }
+};
+
+// A field too large for one SM's shared memory, split by rows over a
+// thread-block cluster of CL CTAs: CTA r holds rows [r*ROWS, (r+1)*ROWS) with
+// the same padded stride.  Row passes stay CTA-local.  A column transform
+// keeps the single-CTA factorisation N = R1*R2: its pass A (R2 points at rows
+// n1 + R1*j) reads and writes every CTA of the cluster through distributed
+// shared memory, each task owned by one thread so that the pass is in place;
+// its pass B (R1 consecutive rows j + R1*k2) is CTA-local because R1 divides
+// ROWS.  The scrambled layout is therefore the single-CTA one.
+template <int N_, int R1_, int NT_, int CL_>
+struct GeoCl : Geo<N_, R1_, NT_, 1> {
+    using Base = Geo<N_, R1_, NT_, 1>;
+    static constexpr int CL = CL_;
+    static constexpr int ROWS = N_ / CL_;
+    static constexpr int FIELD = ROWS * Base::S;
+    static_assert(N_ % CL_ == 0 && ROWS % R1_ == 0, "R1 must divide the rows of one CTA");
+    static_assert(Base::R2 % CL_ == 0 && R1_ % CL_ == 0, "column passes must split over the cluster");
+    __device__ __forceinline__ static int rank() {
+        unsigned r;
+        asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+        return (int)r;
+    }
+    __device__ __forceinline__ static int row0() { return rank() * ROWS; }
 };
 
 // twiddle W_N^{n1 k2} with sign (table holds e^{-2 pi i m/N} as [k2][n1])
@@ -274,10 +304,10 @@ __device__ __forceinline__ float2 twN(const float2 *tw, int n1, int k2) {
 template <class G>
 struct Own {
     static constexpr int W = G::NT / 32;           // warps
-    static constexpr int RPW = G::N / W;            // rows per warp
+    static constexpr int RPW = G::ROWS / W;         // rows per warp
     static constexpr int CPP = 2 * G::N / W;        // columns per warp pair
     static_assert(G::NT % 64 == 0, "NT must be a multiple of 64");
-    static_assert(G::N % W == 0 && (2 * G::N) % W == 0, "rows must split evenly over warps");
+    static_assert(G::ROWS % W == 0 && (2 * G::N) % W == 0, "rows must split evenly over warps");
     __device__ __forceinline__ static int warp() { return threadIdx.x >> 5; }
     __device__ __forceinline__ static int lane() { return threadIdx.x & 31; }
     __device__ __forceinline__ static int pair() { return threadIdx.x >> 6; }
@@ -285,12 +315,34 @@ struct Own {
 };
 
 __device__ __forceinline__ void sync_rows() { __syncwarp(); }
+// barrier of every thread of the cluster, with release / acquire of the
+// shared-memory (local and distributed) and global writes before it
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
 template <class G>
 __device__ __forceinline__ void sync_cols() {
-    // named barrier per warp pair (ids 1..15; 0 is __syncthreads)
-    asm volatile("bar.sync %0, 64;" ::"r"(1 + Own<G>::pair()) : "memory");
+    if constexpr (G::CL > 1) {
+        // the passes on either side touch rows of other CTAs
+        cluster_sync();
+    } else {
+        // named barrier per warp pair (ids 1..15; 0 is __syncthreads)
+        asm volatile("bar.sync %0, 64;" ::"r"(1 + Own<G>::pair()) : "memory");
+    }
+}
+// switch between row and column passes (or any CTA-wide exchange)
+template <class G>
+__device__ __forceinline__ void sync_all() {
+    if constexpr (G::CL > 1) cluster_sync();
+    else __syncthreads();
 }
 __device__ __forceinline__ void sync_all() { __syncthreads(); }
+
+// the same shared-memory offset in CTA r of the cluster (generic address)
+template <class T>
+__device__ __forceinline__ T *peer(T *p, int r) {
+    return cooperative_groups::this_cluster().map_shared_rank(p, (unsigned)r);
+}
 
 struct NoPre {
     static constexpr bool kAhead = false;
@@ -307,7 +359,8 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
     constexpr int TASKS = O::RPW * R1;
-    const int y0 = O::warp() * O::RPW;
+    const int yl0 = O::warp() * O::RPW;  // first local row of the warp
+    const int y0 = G::row0() + yl0;      // its row in the field (pf / op)
     // Pre::kAhead: issue the next task's global loads while the current task
     // runs (double-buffered prefetch); otherwise just before its shared reads
     constexpr bool ahead = Pre::kAhead;
@@ -321,7 +374,7 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
         } else {
             pf(y, n1, pre);
         }
-        float2 *row = buf + y * G::S + n1;
+        float2 *row = buf + (yl0 + tau / R1) * G::S + n1;
         float2 v[R2];
 #pragma unroll
         for (int j = 0; j < R2; ++j) v[j] = row[(R1 + 1) * j];
@@ -374,6 +427,38 @@ template <class G, int SG, bool FWD>
 __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
+    if constexpr (G::CL > 1) {
+        // distributed: CTA r owns the tasks n1 in [r*R1/CL, (r+1)*R1/CL) of
+        // every column; element j (row n1 + R1*j) lives in CTA j / JPC at
+        // local row n1 + R1*(j % JPC)
+        constexpr int JPC = R2 / G::CL;  // elements per CTA
+        constexpr int N1C = R1 / G::CL;  // n1 values per CTA
+        constexpr int TASKS = N1C * G::N;
+        float2 *pb[G::CL];
+#pragma unroll
+        for (int r = 0; r < G::CL; ++r) pb[r] = peer(buf, r);
+        const int n1b = G::rank() * N1C;
+#pragma unroll 1
+        for (int tau = threadIdx.x; tau < TASKS; tau += G::NT) {
+            const int x = tau % G::N, n1 = n1b + tau / G::N;
+            const int off = n1 * G::S + G::px(x);
+            float2 v[R2];
+#pragma unroll
+            for (int j = 0; j < R2; ++j) v[j] = pb[j / JPC][off + R1 * G::S * (j % JPC)];
+            if constexpr (FWD) {
+                DFT<R2, SG>::run(v);
+#pragma unroll
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+            } else {
+#pragma unroll
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+                DFT<R2, SG>::run(v);
+            }
+#pragma unroll
+            for (int j = 0; j < R2; ++j) pb[j / JPC][off + R1 * G::S * (j % JPC)] = v[j];
+        }
+        return;
+    }
     constexpr int TASKS = O::CPP * R1;
     const int x0 = O::pair() * O::CPP;
 #pragma unroll 1
@@ -405,6 +490,27 @@ template <class G, int IN, int OUT, class Op>
 __device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
+    if constexpr (G::CL > 1) {
+        // CTA-local: the R1 rows of task (x, k2) are local rows R1*(k2 - k2b) + j
+        constexpr int K2C = R2 / G::CL;
+        constexpr int TASKS = K2C * G::N;
+        const int k2b = G::rank() * K2C;
+#pragma unroll 1
+        for (int tau = threadIdx.x; tau < TASKS; tau += G::NT) {
+            const int x = tau % G::N, k2l = tau / G::N;
+            const int y0 = R1 * (k2b + k2l);
+            float2 *p = buf + R1 * k2l * G::S + G::px(x);
+            float2 v[R1];
+#pragma unroll
+            for (int j = 0; j < R1; ++j) v[j] = p[G::S * j];
+            if constexpr (IN != 0) DFT<R1, IN>::run(v);
+            op(y0, x, v);
+            if constexpr (OUT != 0) DFT<R1, OUT>::run(v);
+#pragma unroll
+            for (int j = 0; j < R1; ++j) p[G::S * j] = v[j];
+        }
+        return;
+    }
     constexpr int TASKS = O::CPP * R2;
     const int x0 = O::pair() * O::CPP;
 #pragma unroll 1

@@ -1,0 +1,3 @@
+// kernels for 256 x 256 windows: one field over a cluster of 4 CTAs
+#include "mset_kernels_impl.cuh"
+MSET_DEFINE_GEO_CL(256, 16, 512, 4)

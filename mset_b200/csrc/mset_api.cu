@@ -168,8 +168,9 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
     Plan pl;
     if (!plan_for(n, &pl))
         return fail(MSET_E_UNSUPPORTED,
-                    "window size %d has no compiled kernel (supported: 24, 32, 48, 64, 96, 128, 160)", n);
+                    "window size %d has no compiled kernel (supported: 24, 32, 48, 64, 96, 128, 160, 256)", n);
     if (b > nz) b = nz;  // STEP00_INIT.m:126-128
+    if (pl.cl > 1) pl.max_clusters = pl.ops->max_clusters();
     s->plan = pl;
     s->n = n;
     s->nz = nz;
@@ -230,12 +231,15 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
     return 0;
 }
 
-int ensure_save(mset_session *s, int slots) {
+// saved-wave storage for a launch of `grid` CTAs: one slot set per field in
+// flight (per CTA, or per cluster when a field is split over a cluster)
+int ensure_save(mset_session *s, int grid) {
     const size_t per = (size_t)save_slots(s->ns, s->ckpt) * s->n * s->n;
-    if (s->save.n >= per * slots) return 0;
-    cudaError_t e = s->save.ensure(per * slots);
+    const size_t fields = (size_t)std::max(1, grid / std::max(1, s->plan.cl));
+    if (s->save.n >= per * fields) return 0;
+    cudaError_t e = s->save.ensure(per * fields);
     if (e != cudaSuccess) return cuda_fail(e, "allocating saved-wave buffers");
-    s->save_slots = slots;
+    s->save_slots = (int)fields;
     return 0;
 }
 
@@ -291,6 +295,13 @@ int refresh_tilt_table(mset_session *s) {
 }
 
 int persistent_grid(mset_session *s, int items) {
+    const int cl = std::max(1, s->plan.cl);
+    if (cl > 1) {
+        // a field split over a cluster: as many clusters as fit at once
+        int fields = s->plan.max_clusters > 0 ? s->plan.max_clusters : s->sms / cl;
+        if (s->tuned_grid > 0) fields = std::min(fields, s->tuned_grid / cl);
+        return std::max(1, std::min(fields, items)) * cl;
+    }
     if (s->tuned_grid > 0) return std::max(1, std::min(s->tuned_grid, items));
     // CTAs resident per SM for this kernel's shared memory and threads
     const size_t per_sm_smem = 227 * 1024;
@@ -475,7 +486,8 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
     rc = refresh_tilt_table(s);
     if (rc) return rc;
     LaunchArgs a = base_args(s);
-    CKL(launch_positions(s->plan, mode, adjoint, kSeq, a, 1, s->st), "sequential position kernel launch");
+    CKL(launch_positions(s->plan, mode, adjoint, kSeq, a, std::max(1, s->plan.cl), s->st),
+        "sequential position kernel launch");
     TiltBufs &t = s->tilts[0];
     const size_t n2 = (size_t)s->n * s->n;
     CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
@@ -1186,13 +1198,15 @@ int mset_batch_launch_count(mset_session *s) {
 namespace {
 
 int occupancy_limit(const mset_session *s) {
+    if (s->plan.cl > 1) return 1;  // one CTA of a cluster per SM
     const int by_smem = (int)((227 * 1024) / (s->plan.smem + 1024));
     const int by_thr = 2048 / s->plan.nt;
     return std::max(1, std::min(by_smem, by_thr));
 }
 
 double save_bytes(const mset_session *s, int grid, int k) {
-    return (double)grid * save_slots(s->ns, k) * s->n * s->n * sizeof(float2);
+    const int fields = std::max(1, grid / std::max(1, s->plan.cl));
+    return (double)fields * save_slots(s->ns, k) * s->n * s->n * sizeof(float2);
 }
 
 // one warm launch, then `reps` timed launches over the first nitems positions
@@ -1227,8 +1241,12 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
     if (rc) return rc;
     int best_grid = 0, best_k = 0, timed = 0, last_grid = 0;
     double best_us = 0, best_bytes = 0;
+    const int tuned_in = s->tuned_grid;
     for (int c = 1; c <= occ; ++c) {
-        const int grid = std::max(1, std::min(s->sms * c, s->total_pos));
+        s->tuned_grid = 0;
+        const int grid = s->plan.cl > 1 ? persistent_grid(s, s->total_pos)
+                                        : std::max(1, std::min(s->sms * c, s->total_pos));
+        s->tuned_grid = tuned_in;
         if (grid == last_grid) break;
         last_grid = grid;
         for (int k : ks) {
@@ -1328,7 +1346,10 @@ int group_grids(mset_group *g, std::vector<int> &grids) {
     }
     int rc = mset_split_ctas(M, w.data(), occ.data(), g->m[0]->sms, grids.data());
     if (rc) return rc;
-    for (int i = 0; i < M; ++i) grids[i] = std::max(1, std::min(grids[i], std::max(1, g->m[i]->total_pos)));
+    for (int i = 0; i < M; ++i) {
+        const int cl = std::max(1, g->m[i]->plan.cl);
+        grids[i] = std::max(1, std::min(grids[i] / cl, std::max(1, g->m[i]->total_pos))) * cl;
+    }
     return 0;
 }
 

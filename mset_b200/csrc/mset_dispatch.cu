@@ -6,7 +6,7 @@
 
 namespace mset {
 
-#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(96) X(128) X(160)
+#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(96) X(128) X(160) X(256)
 #define X(N_) extern const GeoOps kGeo##N_;
 MSET_GEOS(X)
 #undef X
@@ -25,6 +25,8 @@ bool plan_for(int n, Plan *p) {
     p->n = g->n;
     p->r1 = g->r1;
     p->nt = g->nt;
+    p->cl = g->cl;
+    p->max_clusters = 0;
     p->smem = g->smem;
     p->ctas_per_sm = 0;
     p->ops = g;

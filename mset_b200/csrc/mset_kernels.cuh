@@ -40,7 +40,7 @@ struct LaunchArgs {
     const int2 *items;      // device array of (tilt, position), kBatch/kErr/kSim
     int nitems;
     unsigned *counter;      // work-queue counter (zeroed before the launch)
-    float2 *save;           // per-CTA saved waves: [grid][ns+1][n][n]
+    float2 *save;           // saved waves per field in flight: [fields][slots][n][n]
     const float2 *pscr;     // propagator / N^2, scrambled layout
     const float2 *psep;     // separable propagator: [2n] = (Py / N, Px / N) scrambled, or null
     const float2 *twn;      // [n] twiddles e^{-2 pi i m/N} as [k2][n1]
@@ -50,7 +50,7 @@ struct LaunchArgs {
     float step0, step1, step2;
     int seq_tilt;           // kSeq: index of the tilt to run
     int ckpt;               // 0: keep every slab's wave; k: keep every k-th, recompute the rest
-    int slots;              // saved-wave slots (n x n complex) per CTA
+    int slots;              // saved-wave slots (n x n complex) per field
 };
 
 // saved-wave slots a CTA needs for ns slabs with checkpoint interval k
@@ -63,7 +63,9 @@ __host__ __device__ inline int save_slots(int ns, int k) {
 // per-window-size kernel table (one translation unit per size, geo_<N>.cu)
 struct GeoOps {
     int n, r1, nt;
+    int cl;  // CTAs per field (thread-block cluster size; 1: one CTA per position)
     size_t smem;
+    int (*max_clusters)();  // clusters resident at once (cluster geometries)
     int (*positions)(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st);
     int (*prep_amp)(const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
     int (*prep_amp_bf16)(const float *meas_centred, unsigned short *i_scr, long npos, cudaStream_t st);
@@ -74,6 +76,8 @@ struct GeoOps {
 // host-side launchers (return cudaError_t as int)
 struct Plan {
     int n, r1, nt;
+    int cl;
+    int max_clusters;  // cl > 1: clusters resident at once (0: unknown)
     size_t smem;
     int ctas_per_sm;
     const GeoOps *ops;

@@ -15,6 +15,7 @@
 // (the batched method).  kErr is run_error_mset/_sset (mset.cu:557-810).
 #pragma once
 #include <cuda_bf16.h>
+#include <utility>
 #include "fft_core.cuh"
 #include "mset_kernels.cuh"
 
@@ -91,7 +92,7 @@ struct TSPre {
 // shared-memory layout of the position kernel (float2 units after the field)
 template <class G>
 struct Smem {
-    static constexpr int TW = G::N * G::S, E1 = TW + G::N, E2 = E1 + G::N, PY = E2 + G::N, PX = PY + G::N,
+    static constexpr int TW = G::FIELD, E1 = TW + G::N, E2 = E1 + G::N, PY = E2 + G::N, PX = PY + G::N,
                          END = PX + G::N;
 };
 
@@ -166,7 +167,7 @@ struct PositionKernel {
         sync_rows();
         for (int s = s0; s < s1; ++s) {
             row_passB<G, -1>(buf);
-            sync_all();
+            sync_all<G>();
             col_passA<G, -1, true>(buf, tw);
             sync_cols<G>();
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -175,7 +176,7 @@ struct PositionKernel {
             });
             sync_cols<G>();
             col_passA<G, +1, false>(buf, tw);
-            sync_all();
+            sync_all<G>();
             row_passB<G, +1>(buf);
             sync_rows();
             float2 *o = out + (size_t)(s - s0) * NN;
@@ -229,7 +230,7 @@ struct PositionKernel {
             sincosf(2.0f * MSET_REF_PI * (s2 * nf / (float)N), &sn, &cs);
             e2[L] = make_float2(cs, sn);
         }
-        sync_all();
+        sync_all<G>();
 
         // prefetch of the transmission of slab s for a row-pass task
         auto pf_t = [&](int s) {
@@ -248,7 +249,7 @@ struct PositionKernel {
         });
         sync_cols<G>();
         col_passA<G, -1, false>(buf, tw);
-        sync_all();
+        sync_all<G>();
         row_passB<G, -1>(buf);
         sync_rows();
         row_passA_pf<G, -1, -1, TPre<G>>(buf, tw, pf_t(0), [&](int y, int n1, float2 *v, const TPre<G> &pre) {
@@ -266,7 +267,7 @@ struct PositionKernel {
         if constexpr (METHOD == kMSET) {
             for (int s = 0; s < ns; ++s) {
                 row_passB<G, -1>(buf);
-                sync_all();
+                sync_all<G>();
                 col_passA<G, -1, true>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -275,7 +276,7 @@ struct PositionKernel {
                 });
                 sync_cols<G>();
                 col_passA<G, +1, false>(buf, tw);
-                sync_all();
+                sync_all<G>();
                 row_passB<G, +1>(buf);
                 sync_rows();
                 const bool last = s + 1 == ns;
@@ -308,7 +309,7 @@ struct PositionKernel {
 
         // ---- far field, error, residual (mset.cu:186-227) ----
         row_passB<G, -1>(buf);
-        sync_all();
+        sync_all<G>();
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
         double err = 0.0;
@@ -339,7 +340,7 @@ struct PositionKernel {
                 block_sum2<G::NT>(err, dummy, red);
                 if (threadIdx.x == 0) atomicAdd(t.err, err);
             }
-            sync_all();
+            sync_all<G>();
             return;
         } else {
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -369,13 +370,14 @@ struct PositionKernel {
             if (ck) {
               // park the adjoint state, recompute the waves s0+1 .. s1 of the
               // segment from its checkpoint, restore the state
-              sync_all();
-              for (int i = threadIdx.x; i < N * G::S; i += G::NT) park[i] = buf[i];
-              sync_all();
+              float2 *mine = park + (size_t)G::rank() * G::FIELD;  // this CTA's rows
+              sync_all<G>();
+              for (int i = threadIdx.x; i < G::FIELD; i += G::NT) mine[i] = buf[i];
+              sync_all<G>();
               recompute(a, t, s0, s1, buf, tw, py, px, save + (size_t)seg * NN, recbuf);
-              sync_all();
-              for (int i = threadIdx.x; i < N * G::S; i += G::NT) buf[i] = park[i];
-              sync_all();
+              sync_all<G>();
+              for (int i = threadIdx.x; i < G::FIELD; i += G::NT) buf[i] = mine[i];
+              sync_all<G>();
             }
           }
           for (int s = s1 - 1; s >= s0; --s) {
@@ -386,7 +388,7 @@ struct PositionKernel {
             // the saved wave was written long ago (DRAM); have it in L2 by the row pass
             prefetch_l2(wave, (unsigned)(sizeof(float2) * NN));
             col_passA<G, +1, false>(buf, tw);
-            sync_all();
+            sync_all<G>();
             row_passB<G, +1>(buf);
             sync_rows();
             auto pf = [&](int y, int n1, TSPre<G> &pre) {
@@ -427,7 +429,7 @@ struct PositionKernel {
                 row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop);
                 sync_rows();
                 row_passB<G, -1>(buf);
-                sync_all();
+                sync_all<G>();
                 col_passA<G, -1, true>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -437,7 +439,7 @@ struct PositionKernel {
                 sync_cols<G>();
             } else {
                 row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop);
-                sync_all();
+                sync_all<G>();
             }
           }
         }
@@ -447,9 +449,10 @@ struct PositionKernel {
         //      (mset.cu:316-327; utility.cu:829-876) ----
         double pdx = 0.0, pdy = 0.0;
         if constexpr (ADJ == kREF) {
-            for (int i = threadIdx.x; i < NN; i += G::NT) {
-                const int y = i / N, x = i % N;
-                const float2 c0 = buf[G::at(y, x)];
+            const int yb = G::row0();
+            for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
+                const int yl = i / N, x = i % N, y = yb + yl;
+                const float2 c0 = buf[G::at(yl, x)];
                 const float2 *f = save + (size_t)y * N + x;
                 float2 dx, dy;
                 if (x == 0) dx = csub(f[1], f[0]);
@@ -463,14 +466,14 @@ struct PositionKernel {
                 pdy += (double)(dy.x * c0.x + dy.y * c0.y);
             }
         }
-        sync_all();
+        sync_all<G>();
 
         // ---- probe direction: d = F^{-1}(chi0) fs(-s), accumulated in the
         //      F^{-1}(probe) domain (mset.cu:288-312) ----
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         sync_rows();
         row_passB<G, +1>(buf);
-        sync_all();
+        sync_all<G>();
         col_passA<G, +1, true>(buf, tw);
         sync_cols<G>();
         const float inv = 1.0f / (float)NN;
@@ -506,8 +509,25 @@ struct PositionKernel {
         block_sum2<G::NT>(pdx, pdy, red);
         double dummy = 0.0;
         block_sum2<G::NT>(err, dummy, red);
-        if (threadIdx.x == 0) {
-            atomicAdd(t.err, err);
+        if (threadIdx.x == 0) atomicAdd(t.err, err);
+        if constexpr (G::CL > 1) {
+            // the position sums of every CTA of the cluster, gathered in CTA 0
+            if (threadIdx.x == 0) {
+                double *dst = peer(red + 2 * (G::NT / 32), 0);
+                dst[2 * G::rank()] = pdx;
+                dst[2 * G::rank() + 1] = pdy;
+            }
+            cluster_sync();
+            if (G::rank() == 0 && threadIdx.x == 0) {
+                const double *part = red + 2 * (G::NT / 32);
+                pdx = pdy = 0.0;
+                for (int r = 0; r < G::CL; ++r) {
+                    pdx += part[2 * r];
+                    pdy += part[2 * r + 1];
+                }
+            }
+        }
+        if (G::rank() == 0 && threadIdx.x == 0) {
             if constexpr (MODE == kSeq) {
                 t.sx[p] = sxp + a.step2 * (float)pdx;  // mset.cu:322
                 t.sy[p] = syp + a.step2 * (float)pdy;  // mset.cu:327
@@ -516,7 +536,7 @@ struct PositionKernel {
                 t.posdir[2 * p + 1] = pdy;
             }
         }
-        sync_all();
+        sync_all<G>();
     }
 };
 
@@ -545,18 +565,30 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     // sit in front of every dependent load
     __shared__ TiltDev s_tilt;
     load_tables<G>(buf, a);
-    float2 *save = a.save + (size_t)blockIdx.x * a.slots * G::N * G::N;
-    __syncthreads();
+    // one set of saved-wave slots per field (per cluster when the field is split)
+    float2 *save = a.save + (size_t)(blockIdx.x / G::CL) * a.slots * G::N * G::N;
+    // (cluster) every CTA has started before any distributed shared-memory access
+    sync_all<G>();
     using K = PositionKernel<G, METHOD, ADJ, MODE>;
     if constexpr (MODE == kSeq) {
         if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
-        __syncthreads();
+        sync_all<G>();
         for (int p = 0; p < s_tilt.npos; ++p) K::run(a, s_tilt, p, buf, save, red);
     } else {
         int cur = -1;
         for (;;) {
-            if (threadIdx.x == 0) s_item = (int)atomicAdd(a.counter, 1u);
-            __syncthreads();
+            if constexpr (G::CL > 1) {
+                // CTA 0 of the cluster takes the item and hands it to every CTA
+                if (G::rank() == 0 && threadIdx.x == 0) {
+                    const int v = (int)atomicAdd(a.counter, 1u);
+#pragma unroll
+                    for (int r = 0; r < G::CL; ++r) *peer(&s_item, r) = v;
+                }
+                cluster_sync();
+            } else {
+                if (threadIdx.x == 0) s_item = (int)atomicAdd(a.counter, 1u);
+                __syncthreads();
+            }
             const int it = s_item;
             __syncthreads();
             if (it >= a.nitems) break;
@@ -621,24 +653,26 @@ __global__ void k_prep_prop(const float2 *prop, float2 *pscr) {
     }
 }
 
-// Q = F^{-1}(probe) (scrambled) and probe = F(Q) (natural); one CTA.
+// Q = F^{-1}(probe) (scrambled) and probe = F(Q) (natural); one CTA, or one
+// cluster when the field is split over CTAs.
 template <class G, bool TO_Q>
 __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out, const float2 *twn) {
     extern __shared__ __align__(16) float2 smem[];
     float2 *buf = smem;
-    float2 *tw = buf + G::N * G::S;
+    float2 *tw = buf + G::FIELD;
     for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
-    __syncthreads();
+    sync_all<G>();  // (cluster) every CTA has started before any remote access
     constexpr int N = G::N;
+    const int yb = G::row0();
     if constexpr (TO_Q) {
-        for (int i = threadIdx.x; i < N * N; i += G::NT) buf[G::at(i / N, i % N)] = in[i];
+        for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) buf[G::at(i / N, i % N)] = in[(size_t)yb * N + i];
         __syncthreads();
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         __syncthreads();
         row_passB<G, +1>(buf);
-        __syncthreads();
+        sync_all<G>();
         col_passA<G, +1, true>(buf, tw);
-        __syncthreads();
+        sync_all<G>();
         const float inv = 1.0f / (float)(N * N);
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
@@ -649,9 +683,9 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
 #pragma unroll
             for (int j = 0; j < G::R1; ++j) v[j] = in[(size_t)(y0 + j) * N + x];
         });
-        __syncthreads();
+        sync_all<G>();
         col_passA<G, -1, false>(buf, tw);
-        __syncthreads();
+        sync_all<G>();
         row_passB<G, -1>(buf);
         __syncthreads();
         row_passA<G, -1, 0>(buf, tw, [&](int y, int n1, float2 *v) {
@@ -659,22 +693,71 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
             for (int j = 0; j < G::R2; ++j) out[(size_t)y * N + n1 + G::R1 * j] = v[j];
         });
     }
+    sync_all<G>();  // no CTA leaves while another may still read its shared memory
 }
 
 
 template <class G>
 inline size_t smem_bytes() {
-    return sizeof(float2) * (size_t)Smem<G>::END + sizeof(double) * 2 * ((G::NT + 31) / 32);
+    return sizeof(float2) * (size_t)Smem<G>::END + sizeof(double) * 2 * ((G::NT + 31) / 32 + G::CL);
+}
+
+// launch of `grid` CTAs, in clusters of G::CL when the field is split
+template <class G, class... KA, class... AA>
+inline int launch_geo(void (*k)(KA...), int grid, size_t sm, cudaStream_t st, AA &&...args) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return (int)e;
+    if constexpr (G::CL > 1) {
+        if (grid % G::CL) return (int)cudaErrorInvalidValue;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(G::NT);
+        cfg.dynamicSmemBytes = sm;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = G::CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return (int)cudaLaunchKernelEx(&cfg, k, std::forward<AA>(args)...);
+    } else {
+        k<<<grid, G::NT, sm, st>>>(std::forward<AA>(args)...);
+        return (int)cudaGetLastError();
+    }
 }
 
 template <class G, int METHOD, int ADJ, int MODE>
 inline int launch_one(const LaunchArgs &a, int grid, cudaStream_t st) {
-    auto k = k_positions<G, METHOD, ADJ, MODE>;
-    const size_t sm = smem_bytes<G>();
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return (int)e;
-    k<<<grid, G::NT, sm, st>>>(a);
-    return (int)cudaGetLastError();
+    return launch_geo<G>(k_positions<G, METHOD, ADJ, MODE>, grid, smem_bytes<G>(), st, a);
+}
+
+// clusters of the batched kernel resident at once (0: not a cluster geometry,
+// or the query failed)
+template <class G>
+int geo_max_clusters() {
+    if constexpr (G::CL > 1) {
+        auto k = k_positions<G, kMSET, kREF, kBatch>;
+        const size_t sm = smem_bytes<G>();
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return 0;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(G::CL * 148);
+        cfg.blockDim = dim3(G::NT);
+        cfg.dynamicSmemBytes = sm;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = G::CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) return 0;
+        return n;
+    } else {
+        return 0;
+    }
 }
 
 template <class G>
@@ -711,30 +794,26 @@ int geo_prep_prop(const float *prop, float2 *pscr, cudaStream_t st) {
 template <class G>
 int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cudaStream_t st) {
     const size_t sm = smem_bytes<G>();
-    if (to_q) {
-        auto k = k_probe_q<G, true>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return (int)e;
-        k<<<1, G::NT, sm, st>>>(in, out, twn);
-    } else {
-        auto k = k_probe_q<G, false>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return (int)e;
-        k<<<1, G::NT, sm, st>>>(in, out, twn);
-    }
-    return (int)cudaGetLastError();
+    if (to_q) return launch_geo<G>(k_probe_q<G, true>, G::CL, sm, st, in, out, twn);
+    return launch_geo<G>(k_probe_q<G, false>, G::CL, sm, st, in, out, twn);
 }
 
 }  // namespace mset
 
 // one translation unit per window size defines its table entry
-#define MSET_DEFINE_GEO(N_, R1_, NT_, MINB_)                                           \
+#define MSET_DEFINE_GEO(N_, R1_, NT_, MINB_) MSET_DEFINE_GEO_T(N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
+// a field split by rows over a cluster of CL_ CTAs
+#define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
+#define MSET_UNPAREN(...) __VA_ARGS__
+#define MSET_DEFINE_GEO_T(N_, R1_, GT_)                                                \
     namespace mset {                                                                   \
-    using Geo##N_ = Geo<N_, R1_, NT_, MINB_>;                                               \
+    using Geo##N_ = MSET_UNPAREN GT_;                                                  \
     extern const GeoOps kGeo##N_ = {N_,                                                \
                                     R1_,                                               \
-                                    NT_,                                               \
+                                    Geo##N_::NT,                                       \
+                                    Geo##N_::CL,                                       \
                                     smem_bytes<Geo##N_>(),                             \
+                                    &geo_max_clusters<Geo##N_>,                        \
                                     &geo_positions<Geo##N_>,                           \
                                     &geo_prep_amp<Geo##N_>,                            \
                                     &geo_prep_amp_bf16<Geo##N_>,                       \

@@ -24,8 +24,11 @@ def pos_tol(n: int) -> float:
     factors sum|t|/|sum t| of ~1e3; FP32 propagation limits them to ~1e-4 at
     N <= 96 and ~4e-4 at N = 160.  On the same inputs the reference's own FP32
     CUDA code (float host sums, utility.cu:928-942) deviates from the FP64
-    oracle by 2-3x more (measured 2.7e-4 at N = 128, 9.5e-4 at N = 160)."""
-    return TOL if n <= 96 else 5e-4
+    oracle by 2-3x more (measured 2.7e-4 at N = 128, 9.5e-4 at N = 160).  At
+    N = 256 the updated coordinates (~128 px, float32 ulp 1.5e-5) differ from
+    their start by 0.01-0.1 px, so storage alone resolves the change to a
+    few 1e-4; measured 1.5e-3."""
+    return TOL if n <= 96 else (5e-4 if n <= 160 else 2e-3)
 
 
 def _steps(c, method, admode=0):
@@ -39,6 +42,7 @@ CASES = [
     dict(n=128, nz=4, npos=3, b=2),
     dict(n=96, nz=3, npos=3, b=1),
     dict(n=160, nz=3, npos=2, b=1),
+    dict(n=256, nz=3, npos=2, b=1),  # field split over a 4-CTA cluster
 ]
 
 
@@ -78,7 +82,7 @@ def test_error_pass_matches_oracle(gpu_available, method):
 
 @pytest.mark.parametrize("admode", [MSET_ADJOINT_REF, MSET_ADJOINT_EXACT], ids=["ref", "exact"])
 @pytest.mark.parametrize("method", [MSET_MODE_MSET, MSET_MODE_SSET], ids=["mset", "sset"])
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [64, 128, 256])
 def test_batched_gradient_matches_oracle(gpu_available, admode, method, n):
     tilts = [small_case(n=n, nz=6, npos=5, b=2, seed=20 + j, defocus=15.0, jitter=6.0, strength=STRENGTH)
              for j in range(2)]
@@ -94,8 +98,36 @@ def test_batched_gradient_matches_oracle(gpu_available, admode, method, n):
                                       sigma=c0["sigma"], dz=c0["dz"], binning=2, method=method, adjoint=admode)
         assert rel_l2(out["grad"][j], g) < TOL
         assert rel_l2(np.fft.fft2(out["probe"][j]), pa) < TOL
-        assert rel_l2(out["posdir"][5 * j:5 * j + 5], pd) < (TOL if n <= 96 else 3e-4)
+        assert rel_l2(out["posdir"][5 * j:5 * j + 5], pd) < (TOL if n <= 96 else 3e-4 if n <= 160 else pos_tol(n))
         assert abs(out["err"][j] - e) <= TOL * e
+
+
+def test_cluster_window_simulate_checkpoint_and_probe(gpu_available):
+    """256^2 window (one field over a 4-CTA cluster): far-field intensities,
+    checkpointed pass (k = 2) against full storage and the oracle, and the
+    probe round trip through the scrambled F^{-1}(probe) domain"""
+    n = 256
+    c = small_case(n=n, nz=6, npos=3, b=1, seed=61, defocus=15.0, jitter=6.0, strength=STRENGTH)
+    bs = BatchSession(n=n, nz=6, npos=[3], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+    bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"], volume=c["V"])
+    _, pr, _, _ = bs.get_tilt(0)
+    assert rel_l2(pr, c["probe"]) < 1e-5
+    I = bs.simulate()
+    for p in range(3):
+        o = O.position(c["V"], c["probe"], c["prop"], c["sx"][p], c["sy"][p], O.amp_std(c["meas"][p]),
+                       sigma=c["sigma"], dz=c["dz"])
+        assert rel_l2(I[p], np.fft.fftshift(np.abs(o["far"]) ** 2)) < TOL
+    full = bs.gradient()
+    bs.set_checkpoint(2)
+    ck = bs.gradient()
+    bs.close()
+    for key in ("grad", "probe", "posdir", "err"):
+        assert rel_l2(ck[key], full[key]) < 1e-9, key
+    g, pa, pd, e = O.batched_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"], sigma=c["sigma"],
+                                  dz=c["dz"], binning=1)
+    assert rel_l2(ck["grad"][0], g) < TOL
+    assert rel_l2(np.fft.fft2(ck["probe"][0]), pa) < TOL
+    assert abs(ck["err"][0] - e) <= TOL * e
 
 
 def test_simulate_matches_oracle_far_field(gpu_available):
