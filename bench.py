@@ -121,6 +121,8 @@ def build_problem(cfg_name: str, rank: int, device: int, method: int = 1, adjoin
     bs = BatchSession(n=cfg.window, nz=cfg.vol[0], npos=npos, prop=spec.prop, sigma=spec.sigma,
                       potential_pixelsize=cfg.dx, slice_binning=cfg.slice_binning, method=method,
                       adjoint=adjoint, device=device)
+    if cfg.name.startswith("large"):
+        bs.set_amplitude_bf16(True)  # measured counts stored as BF16 (22 GB instead of 44 GB at 41 tilts)
     # simulate the measured intensities with the library's own forward model
     for j, v in enumerate(spec.volumes):
         bs.set_tilt(j, probe=spec.probe, scan_x=spec.scan_x, scan_y=spec.scan_y,
@@ -137,6 +139,14 @@ def build_problem(cfg_name: str, rank: int, device: int, method: int = 1, adjoin
         bs.set_tilt(j, measured=meas[off:off + npos[j]], volume=0.5 * v)
         off += npos[j]
     return cfg, spec, bs, meas
+
+
+def workload_name(cfg, ns: int, positions: int) -> str:
+    nz, ny, nx = cfg.vol
+    vol = f"{nx}^3" if nx == ny == nz else f"{nx}x{ny}x{nz}"
+    return (f"{cfg.name}: {vol} volume, {cfg.window}^2 window, {cfg.scan[0]}x{cfg.scan[1]} scan, "
+            f"{cfg.n_tilts} tilts, {ns} slabs x {cfg.slice_binning} voxels, batched gradient pass over all "
+            f"{positions} positions")
 
 
 def run_ours(args):
@@ -165,6 +175,7 @@ def run_ours(args):
     if rank == 0:
         sampler.start()
     ms = bs.time_gradient(args.steps)  # CUDA events on the session stream, K passes
+    meas_bytes = positions * n * n * (2 if cfg.name.startswith("large") else 4)
     torch.cuda.synchronize()
     clocks = sampler.stop() if rank == 0 else {}
     t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -176,7 +187,8 @@ def run_ours(args):
     # full batched iteration as one CUDA graph: rotate -> forward -> loss ->
     # adjoint -> rotate back -> update -> positivity -> TV-FISTA (lambda 1e-3)
     it_ms = None
-    if not args.no_iter:
+    cubic = cfg.vol[0] == cfg.vol[1] == cfg.vol[2] and cfg.vol[0] <= 160
+    if not args.no_iter and cubic:
         bs.iteration_setup(cfg.vol[0], spec.angles, positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter,
                            tv_fista=True)
         bs.set_rec(0.5 * spec.lab)
@@ -249,16 +261,17 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "fp32 (complex64 propagation, fp64 reductions)",
             "data": "synthetic (seeded fcc Cu/Au-like Gaussian-atom lattice, Poisson 1e4 e-/probe)",
-            "config": {"workload": "mid: 128^3 volume, 128^2 window, 32x32 scan, 21 tilts, 64 slabs x 2 voxels, "
-                                   "batched gradient pass over all 21504 positions",
+            "config": {"workload": workload_name(cfg, ns, positions),
                        "positions_per_gpu": positions, "slabs": ns, "window": n,
-                       "units_per_step_per_gpu": units, "l2": "inputs larger than L2 (1.4 GB amplitudes)",
+                       "units_per_step_per_gpu": units, "persistent_ctas": bs.shape()["grid"],
+                       "l2": f"inputs larger than L2 ({meas_bytes / 1e9:.1f} GB measured patterns)",
                        "parallelism": f"tilt replicas x{world}"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak,
                          # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_positions launch on
                          # the mid_s capture (128 positions: 1.0775 GB + 1.1117 GB), scaled by units
-                         "traffic": TRAFFIC_PER_UNIT * units,
+                         # (n^2 scaling to other windows: both terms are per-pixel)
+                         "traffic": TRAFFIC_PER_UNIT * units * (n / 128.0) ** 2,
                          "traffic_note": "bytes per launch from the ncu capture of the same kernel on 128 positions "
                                          "(profiles/k_positions_mid_s.md), scaled by slice-propagations; "
                                          "algorithmic bytes per unit 16*n^2 (saved wave write + read) + "

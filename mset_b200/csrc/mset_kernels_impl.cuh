@@ -79,7 +79,8 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
 
 template <class G>
 struct TPre {
-    static constexpr bool kAhead = true;
+    // double buffer only while the register budget allows it (R2 <= 8)
+    static constexpr bool kAhead = G::R2 <= 8;
     float2 t[G::R2];  // transmission of the task's elements
 };
 template <class G>
@@ -104,6 +105,9 @@ struct PositionKernel {
     // (mset.cu:134-153 / STEP02_FORWARD_4D.m:12-20; SSET: all z, mset.cu:391-404),
     // read from the precomputed slabs when the tilt has them
     static __device__ __forceinline__ float2 trans(const LaunchArgs &a, const TiltDev &t, int s, int y, int x) {
+        // batched passes always run on precomputed slabs
+        if constexpr (MODE == kBatch || MODE == kBatchCk || MODE == kSim)
+            return t.T[(size_t)s * NN + (size_t)y * N + x];
         if (t.T) return t.T[(size_t)s * NN + (size_t)y * N + x];
         int z0, z1;
         if constexpr (METHOD == kSSET) {
@@ -204,7 +208,7 @@ struct PositionKernel {
         }
     }
 
-    static __device__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, float2 *save,
+    static __device__ __forceinline__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, float2 *save,
                                double *red) {
         const float2 *tw = buf + Smem<G>::TW;
         float2 *e1 = buf + Smem<G>::E1;

@@ -57,6 +57,14 @@ CONFIGS = {
     # +-5 nm defocus and C3 = 1 mm +- 1 um probe errors and +-0.5 px jitter
     "grad": Config("grad", (24, 24, 24), 0.4, 128, (12, 12), 2.0, 5, 30.0, 1, 1e4,
                    defocus_A=50.0, C30_A=1e7, jitter_px=0.5),
+    # large single reconstruction: 256x256x192 at 0.25 A, 256^2 window (one
+    # field over a 4-CTA cluster), 64x64 scan at 4 px, 41 tilts over +-70 deg,
+    # 96 slices of 2 voxels
+    "large": Config("large", (192, 256, 256), 0.25, 256, (64, 64), 4.0, 41, 70.0, 2, 1e4),
+    # its geometry on 3 of the tilts (-70, 0, +70 deg), for timing samples
+    "large_s": Config("large_s", (192, 256, 256), 0.25, 256, (64, 64), 4.0, 3, 70.0, 2, 1e4),
+    # its geometry on 1 tilt x 12x12 positions, for profiling captures
+    "large_p": Config("large_p", (192, 256, 256), 0.25, 256, (12, 12), 4.0, 1, 0.0, 2, 1e4),
 }
 
 # uneven-size batch: 6 independent tilt series run as one pass, windows 64^2 to
