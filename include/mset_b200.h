@@ -259,6 +259,20 @@ int mset_batch_get_rec(mset_session *s, float *rec);
 /* niter iterations; err_out [niter][ntilts] (sum of (A-M)^2 of the pass before
  * each update), tv_err_out [niter]; both nullable */
 int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_out, double *tv_err_out);
+/* niter iterations with the backtracking line search of the reference's
+ * reconstruction loop (Run_MSET_recon.m:106-252): each iteration saves rec,
+ * probes and positions, applies one update without TV, runs the error pass of
+ * the new state (mean over tilts of err / positions / n^2, mex_main.cu:179);
+ * if that is not below the previous iteration's mean error (1e31 at the
+ * start) the state is restored and all three step sizes are multiplied by
+ * bls_parameter, until the object step falls below bls_parameter^5 times its
+ * value at the call (then the call stops early, state restored).  After an
+ * accepted update, TV as configured.  The session's step sizes stay reduced.
+ * mean_err_out [niter] and step_out [niter][3] (nullable) hold the accepted
+ * iterations' errors and step sizes; iters_out (nullable) their count.
+ * Host-driven: one host synchronisation per trial. */
+int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, double *mean_err_out,
+                           float *step_out, int *iters_out);
 /* captures the iteration graph, then times niter replays with CUDA events on
  * the session stream (the state advances by niter iterations) */
 int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter);

@@ -58,6 +58,7 @@ SIGNATURES = {
     "mset_batch_set_rec": (C.c_int, [C.c_void_p, _F]),
     "mset_batch_get_rec": (C.c_int, [C.c_void_p, _F]),
     "mset_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D]),
+    "mset_batch_iterate_bls": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _D, _F, C.POINTER(C.c_int)]),
     "mset_batch_iterate_time": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "mset_batch_iterate_phase": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "mset_batch_device_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),

@@ -167,6 +167,17 @@ class BatchSession:
         check("mset_batch_iterate", self._lib.mset_batch_iterate(self._h, int(niter), int(use_graph), dptr(e), dptr(t)))
         return e[:niter], t[:niter]
 
+    def iterate_bls(self, niter: int, bls_parameter: float = 0.5):
+        """iterations with the reference's backtracking line search
+        (mset_batch_iterate_bls); returns (mean errors, step sizes) of the
+        accepted iterations"""
+        e = np.zeros(max(niter, 1))
+        st = np.zeros((max(niter, 1), 3), np.float32)
+        k = C.c_int()
+        check("mset_batch_iterate_bls", self._lib.mset_batch_iterate_bls(
+            self._h, int(niter), float(bls_parameter), dptr(e), fptr(st), C.byref(k)))
+        return e[:k.value], st[:k.value]
+
     def time_iteration(self, niter: int) -> float:
         ms = np.zeros(1)
         check("mset_batch_iterate_time", self._lib.mset_batch_iterate_time(self._h, int(niter), dptr(ms)))

@@ -343,6 +343,21 @@ template <class T>
 __device__ __forceinline__ T *peer(T *p, int r) {
     return cooperative_groups::this_cluster().map_shared_rank(p, (unsigned)r);
 }
+// shared::cluster window address of a local shared-memory pointer in CTA r
+__device__ __forceinline__ uint32_t peer_addr(const void *p, int r) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(a), "r"(r));
+    return out;
+}
+__device__ __forceinline__ float2 ld_cluster(uint32_t addr) {
+    float2 v;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, float2 v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
 
 struct NoPre {
     static constexpr bool kAhead = false;
@@ -434,17 +449,18 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
         constexpr int JPC = R2 / G::CL;  // elements per CTA
         constexpr int N1C = R1 / G::CL;  // n1 values per CTA
         constexpr int TASKS = N1C * G::N;
-        float2 *pb[G::CL];
+        uint32_t pb[G::CL];  // shared::cluster addresses of the CTAs' fields
 #pragma unroll
-        for (int r = 0; r < G::CL; ++r) pb[r] = peer(buf, r);
+        for (int r = 0; r < G::CL; ++r) pb[r] = peer_addr(buf, r);
         const int n1b = G::rank() * N1C;
+        constexpr uint32_t kRow = sizeof(float2) * R1 * G::S;  // bytes between elements j, j+1 of one CTA
 #pragma unroll 1
         for (int tau = threadIdx.x; tau < TASKS; tau += G::NT) {
             const int x = tau % G::N, n1 = n1b + tau / G::N;
-            const int off = n1 * G::S + G::px(x);
+            const uint32_t off = sizeof(float2) * (uint32_t)(n1 * G::S + G::px(x));
             float2 v[R2];
 #pragma unroll
-            for (int j = 0; j < R2; ++j) v[j] = pb[j / JPC][off + R1 * G::S * (j % JPC)];
+            for (int j = 0; j < R2; ++j) v[j] = ld_cluster(pb[j / JPC] + off + kRow * (j % JPC));
             if constexpr (FWD) {
                 DFT<R2, SG>::run(v);
 #pragma unroll
@@ -455,7 +471,7 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
                 DFT<R2, SG>::run(v);
             }
 #pragma unroll
-            for (int j = 0; j < R2; ++j) pb[j / JPC][off + R1 * G::S * (j % JPC)] = v[j];
+            for (int j = 0; j < R2; ++j) st_cluster(pb[j / JPC] + off + kRow * (j % JPC), v[j]);
         }
         return;
     }

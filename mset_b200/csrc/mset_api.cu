@@ -121,6 +121,8 @@ struct mset_session {
     int nv = 0;
     std::vector<RotPlan> plan_inv, plan_fwd;
     DevBuf<float> rec, gvol;
+    DevBuf<float> bls_rec, bls_pos;  // line search: state before the tried update
+    DevBuf<float2> bls_q;
     DevBuf<double> gacc, err_hist, tv_hist;
     DevBuf<unsigned> it_counter, mx_bits;
     DevBuf<float> mx;
@@ -972,7 +974,7 @@ int mset_batch_get_rec(mset_session *s, float *rec) {
 // volumes, the batched pass and the lab-frame gradient sum over this
 // session's tilts (gacc); phase 2: the update from gacc.  A caller that
 // shards tilts over GPUs all-reduces gacc between the phases.
-static int record_phase(mset_session *s, int phase) {
+static int record_phase(mset_session *s, int phase, bool with_tv = true, bool with_hist = true) {
     const int J = (int)s->tilts.size();
     const int nv = s->nv, n = s->n;
     const long V = (long)nv * nv * nv;
@@ -1009,7 +1011,7 @@ update:
     // 4. object update, positivity (Run_MSET_recon.m:183-185), TV (:267-270)
     CKL(vol_update(s->rec.p, s->gacc.p, V, s->step[0], s->st), "update");
     if (s->it_pos) CKL(vol_positivity(s->rec.p, V, s->st), "positivity");
-    if (s->it_tv) {
+    if (s->it_tv && with_tv) {
         CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
         CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
         CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
@@ -1020,6 +1022,7 @@ update:
     }
     // 5. probe and scan positions
     CKL(launch_apply_probe_pos(s->h_tilts.data(), J, n, s->step[1], s->step[2], s->st), "apply");
+    if (!with_hist) return 0;
     // 6. error history
     k_record_err<<<1, 64, 0, s->st>>>(s->err.p, J, s->err_hist.p, s->hist_cap, s->it_counter.p,
                                       s->it_tv ? s->tv_err.p : nullptr, s->tv_hist.p);
@@ -1081,6 +1084,67 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
     return 0;
 }
 
+// TV / TV-FISTA of rec / max(rec), rescaled by max(rec) (Run_MSET_recon.m:267-270)
+static int record_tv(mset_session *s) {
+    const int nv = s->nv;
+    const long V = (long)nv * nv * nv;
+    CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
+    CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
+    CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
+    const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
+                    s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
+    CKL(tv_prox(ta, s->st), "tv");
+    CKL(vol_mul(s->tv_out.p, s->rec.p, V, s->mx.p, s->st), "rescale");
+    return 0;
+}
+
+// error pass of the current state over every tilt: V_j = pad(Func_inv_rot(rec)),
+// forward only (run_error_mset, mset.cu:557-696), sums into s->err
+static int record_error_phase(mset_session *s) {
+    const int J = (int)s->tilts.size();
+    const int nv = s->nv, n = s->n;
+    const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
+    const int bvox = s->method == MSET_MODE_SSET ? s->nz : s->b;
+    for (int j = 0; j < J; ++j) {
+        CKL(rot_apply(s->plan_inv[j], nv, s->rec.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
+        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, nv, n, s->st), "pad");
+    }
+    CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * J, s->st));
+    CKL(launch_transmission(s->d_tilts.p, J, n, s->nz, bvox, nsg, s->sigma * s->dz, s->st), "transmission");
+    CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
+    LaunchArgs la = base_args(s);
+    CKL(launch_positions(s->plan, s->method, kREF, kErr, la, s->grid_cache, s->st), "error pass");
+    return 0;
+}
+
+// copy of the state a line-search step may have to undo: rec, probes, positions
+static int bls_state(mset_session *s, bool save) {
+    const size_t n2 = (size_t)s->n * s->n;
+    const long V = (long)s->nv * s->nv * s->nv;
+    if (save) CK(cudaMemcpyAsync(s->bls_rec.p, s->rec.p, sizeof(float) * V, cudaMemcpyDeviceToDevice, s->st));
+    else CK(cudaMemcpyAsync(s->rec.p, s->bls_rec.p, sizeof(float) * V, cudaMemcpyDeviceToDevice, s->st));
+    for (size_t j = 0; j < s->tilts.size(); ++j) {
+        TiltBufs &t = s->tilts[j];
+        float2 *q = s->bls_q.p + j * n2;
+        float *px = s->bls_pos.p + 2 * (size_t)s->pos_off[j], *py = px + t.npos;
+        const size_t pb = sizeof(float) * t.npos;
+        if (save) {
+            CK(cudaMemcpyAsync(q, t.Q.p, sizeof(float2) * n2, cudaMemcpyDeviceToDevice, s->st));
+            if (t.npos) {
+                CK(cudaMemcpyAsync(px, t.sx.p, pb, cudaMemcpyDeviceToDevice, s->st));
+                CK(cudaMemcpyAsync(py, t.sy.p, pb, cudaMemcpyDeviceToDevice, s->st));
+            }
+        } else {
+            CK(cudaMemcpyAsync(t.Q.p, q, sizeof(float2) * n2, cudaMemcpyDeviceToDevice, s->st));
+            if (t.npos) {
+                CK(cudaMemcpyAsync(t.sx.p, px, pb, cudaMemcpyDeviceToDevice, s->st));
+                CK(cudaMemcpyAsync(t.sy.p, py, pb, cudaMemcpyDeviceToDevice, s->st));
+            }
+        }
+    }
+    return 0;
+}
+
 static void drop_phase_graphs(mset_session *s) {
     for (int p = 0; p < 2; ++p) {
         if (s->phase_exec[p]) cudaGraphExecDestroy(s->phase_exec[p]);
@@ -1088,6 +1152,76 @@ static void drop_phase_graphs(mset_session *s) {
         s->phase_exec[p] = nullptr;
         s->phase_graph[p] = nullptr;
     }
+}
+
+int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, double *mean_err_out,
+                           float *step_out, int *iters_out) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
+    if (niter < 0) return fail(MSET_E_ARG, "niter < 0");
+    if (!(bls_parameter > 0.0 && bls_parameter < 1.0)) return fail(MSET_E_ARG, "bls_parameter must be in (0, 1)");
+    if (iters_out) *iters_out = 0;
+    const int J = (int)s->tilts.size();
+    const size_t n2 = (size_t)s->n * s->n;
+    const long V = (long)s->nv * s->nv * s->nv;
+    const int grid = persistent_grid(s, std::max(1, s->total_pos));
+    rc = ensure_save(s, grid);
+    if (rc) return rc;
+    s->grid_cache = grid;
+    rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    CK(s->bls_rec.ensure(V));
+    CK(s->bls_q.ensure(std::max<size_t>(1, n2 * J)));
+    CK(s->bls_pos.ensure(std::max<size_t>(1, 2 * (size_t)s->total_pos)));
+    // the step sizes change below: graphs captured with the old ones are stale
+    drop_graph(s);
+    const float step0_orig = s->step[0];
+    const double floor0 = std::pow(bls_parameter, 5) * (double)step0_orig;
+    double old_mean = 1e31;
+    std::vector<double> err(J);
+    int done = 0;
+    bool stop = false;
+    for (int i = 0; i < niter && !stop; ++i) {
+        rc = bls_state(s, true);
+        if (rc) return rc;
+        double mean = 0;
+        for (;;) {
+            // one update (rotations, pass, gradient sum, update, positivity,
+            // probe and position steps), then the error of the new state
+            rc = record_phase(s, 1);
+            if (!rc) rc = record_phase(s, 2, false, false);
+            if (!rc) rc = record_error_phase(s);
+            if (rc) return rc;
+            CK(cudaMemcpyAsync(err.data(), s->err.p, sizeof(double) * J, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            mean = 0;
+            for (int j = 0; j < J; ++j)
+                mean += s->npos[j] ? err[j] / s->npos[j] / (double)n2 : 0.0;  // mex_main.cu:179
+            mean /= J;
+            if (old_mean > mean) break;                 // accepted (Run_MSET_recon.m:240)
+            rc = bls_state(s, false);                   // rejected: undo, shrink every step
+            if (rc) return rc;
+            for (int k = 0; k < 3; ++k) s->step[k] = (float)(bls_parameter * s->step[k]);
+            if ((double)s->step[0] < floor0) {          // Run_MSET_recon.m:250-253
+                stop = true;
+                break;
+            }
+        }
+        if (stop) break;
+        if (s->it_tv) {
+            rc = record_tv(s);
+            if (rc) return rc;
+        }
+        if (mean_err_out) mean_err_out[i] = mean;
+        if (step_out)
+            for (int k = 0; k < 3; ++k) step_out[3 * i + k] = s->step[k];
+        old_mean = mean;
+        ++done;
+    }
+    CK(cudaStreamSynchronize(s->st));
+    if (iters_out) *iters_out = done;
+    return 0;
 }
 
 int mset_batch_iterate_phase(mset_session *s, int phase, int use_graph) {

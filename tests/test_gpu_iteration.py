@@ -109,3 +109,42 @@ def test_phase_split_equals_full_iteration(gpu_available):
     assert rel_l2(outs[1][0] - rec0, outs[0][0] - rec0) < 1e-6
     for a, c in zip(outs[0][1], outs[1][1]):
         assert rel_l2(a, c) < 1e-6
+
+
+def test_line_search_matches_oracle(gpu_available):
+    """the reference's backtracking line search (Run_MSET_recon.m:106-252) on
+    the batched iteration: steps 4x too large, so the second iteration rejects
+    two trials before it accepts; accepted errors, step sizes, volume, probes
+    and positions against the FP64 oracle of the same rule"""
+    nv, n, b, dz, sigma, prop, angles, tilts, rec0 = _problem()
+    V0 = IO.pad(O.rot3d(rec0, angles[1], inverse=True), n).astype(np.float32)
+    g, pa, pd, _ = O.batched_tilt(V0, tilts[1]["probe"], prop, tilts[1]["sx"], tilts[1]["sy"], tilts[1]["meas"],
+                                  sigma=sigma, dz=dz, binning=b)
+    step = 4.0 * np.array([0.05 * rec0.max() / np.abs(g).max(),
+                           0.01 * np.abs(tilts[1]["probe"]).max() / np.abs(pa).max(), 0.1 / np.abs(pd).max()])
+    step = step.astype(np.float32)
+    rec_o, tl, e_o, st_o = IO.iterate_bls(rec0.astype(np.float64), [dict(t) for t in tilts], prop, angles,
+                                          sigma=sigma, dz=dz, binning=b, step=step, bls=0.5, niter=4,
+                                          tv_lambda=0.02, tv_iter=20)
+    assert len(e_o) == 4 and st_o[-1][0] < step[0]  # the rule did reject
+
+    bs = BatchSession(n=n, nz=nv, npos=[4, 4, 4], prop=prop, sigma=sigma, potential_pixelsize=dz, slice_binning=b,
+                      step_size=step)
+    for j, t in enumerate(tilts):
+        bs.set_tilt(j, probe=t["probe"], scan_x=t["sx"], scan_y=t["sy"], measured=t["meas"])
+    bs.iteration_setup(nv, angles, positivity=True, tv_lambda=0.02, tv_iter=20, tv_fista=True)
+    bs.set_rec(rec0)
+    e_g, st_g = bs.iterate_bls(4, 0.5)
+    rec_g = bs.get_rec()
+    probes_g = [bs.get_tilt(j)[1] for j in range(3)]
+    pos_g = [bs.get_tilt(j)[2:] for j in range(3)]
+    bs.close()
+    np.testing.assert_array_equal(st_g, np.asarray(st_o, np.float32))
+    assert rel_l2(e_g, e_o) < 1e-4
+    assert rel_l2(rec_g - rec0, rec_o - rec0) < 1e-4
+    for j in range(3):
+        assert rel_l2(probes_g[j] - tilts[j]["probe"], tl[j]["probe"] - tilts[j]["probe"]) < 1e-4
+        d_g = np.r_[pos_g[j][0] - tilts[j]["sx"], pos_g[j][1] - tilts[j]["sy"]]
+        d_o = np.r_[tl[j]["sx"] - tilts[j]["sx"], tl[j]["sy"] - tilts[j]["sy"]]
+        # four accepted iterations of cancellation-limited position sums
+        assert rel_l2(d_g, d_o) < 3e-4
