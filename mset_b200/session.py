@@ -82,6 +82,16 @@ class Session:
                                                                  int(bool(inverse))))
         return out
 
+    def tv(self, vol, lam: float, niter: int, fista: bool = False):
+        """TV_method (fista=False) / TV_FISTA_method of a [n3][n2][n1] volume
+        (mset_tv); returns the regularised volume"""
+        out = np.array(_c32(vol), dtype=np.float32, copy=True)
+        n3, n2, n1 = out.shape
+        err = np.zeros(1)
+        check("mset_tv", self._lib.mset_tv(self._h, fptr(out), n1, n2, n3, float(lam), int(niter), int(bool(fista)),
+                                           err.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     # ---- 'upload' (mex_main.cu:42-95) ----
     def upload(self, rvol, probe, prop, *, sigma: float, potential_pixelsize: float,
                scan_x, scan_y, measured, step_size=(0.0, 0.0, 0.0), slice_binning: int = 1,
