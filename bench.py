@@ -10,6 +10,12 @@ adjoint with V / probe / scan-position gradients of every position of every
 tilt, in one persistent launch.  Inputs (measured amplitudes 1.4 GB) exceed
 L2, so no flush is needed between steps.
 
+Beside the headline (rank 0, mid workload only; --no-* skips them): the full
+iteration as one CUDA graph, the sequential plain forms (this library's and
+the reference's own CUDA module), the uneven-size 6-series group pass with the
+autotuner, the 256^2-window cluster kernel on 3 tilts of the large geometry,
+and the FP64 CPU port on a sample.
+
 One JSON line on stdout (rank 0).  --impl reference times the FP64 CPU port
 of the reference's path (the reference's own CPU path is MATLAB code, which
 is not available here) on a bounded sample of the same workload.
@@ -219,7 +225,9 @@ def run_ours(args):
     # updating volume, probe and position; mset_run) and the reference's own
     # CUDA module (oracle/_ref, cuFFT) on a sample of the same tilt
     plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (rank == 0 and not args.no_plain) else None
-    uneven = uneven_batch(args, local) if (rank == 0 and args.uneven) else None
+    side = rank == 0 and args.config == "mid"
+    uneven = uneven_batch(args, local) if (side and not args.no_uneven) else None
+    large = large_window(args, local) if (side and not args.no_large) else None
 
     # end to end through the C ABI with host buffers: volumes in, gradients out
     vols = [np.ascontiguousarray(0.5 * v) for v in spec.volumes]
@@ -291,6 +299,7 @@ def run_ours(args):
                 "slice_propagations_per_s": world * units / (it_ms / 1e3)},
             "plain_forms": plain,
             "uneven_batch": uneven,
+            "large_window": large,
             "gpu_launches": args.steps * bs._lib.mset_batch_launch_count(bs._h),
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -406,6 +415,32 @@ def uneven_batch(args, device: int) -> dict:
             "what": "6 tilt series of uneven size in one CUDA-graph group pass, shapes and schedule autotuned"}
 
 
+def large_window(args, device: int) -> dict:
+    """The large-reconstruction geometry (256^2 window split over a 4-CTA
+    cluster, 256x256x192 volume, 96 slabs, BF16 counts) on 3 of its 41 tilts:
+    the batched gradient pass, device-timed."""
+    import torch
+
+    cfg, spec, bs, meas = build_problem("large_s", 0, device)
+    del meas
+    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    units = int(bs.npos.sum()) * ns
+    for _ in range(max(args.warmup, 1)):
+        bs.gradient(want=())
+    torch.cuda.synchronize()
+    ms = bs.time_gradient(max(1, min(args.steps, 3)))
+    n = cfg.window
+    flop = units * flops_per_unit(n) + int(bs.npos.sum()) * flops_per_position(n)
+    peaks = measured_peaks()
+    fp32_peak = 148 * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    out = {"value": units / (ms / 1e3), "unit": "slice-propagations/s", "ms_per_pass": ms,
+           "units_per_pass": units, "workload": workload_name(cfg, ns, int(bs.npos.sum())),
+           "persistent_ctas": bs.shape()["grid"], "measured_storage": "bf16",
+           "fp32_frac": flop / (ms / 1e3) / 1e12 / fp32_peak}
+    bs.close()
+    return out
+
+
 def cpu_sample_positions(cores: int) -> int:
     return int(max(8, min(96, 6 * cores)))
 
@@ -490,7 +525,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the sequential-form timings")
     ap.add_argument("--plain-positions", type=int, default=32, help="positions in the sequential-form sample")
     ap.add_argument("--tv-iter", type=int, default=300, help="TV-FISTA inner iterations per iteration")
-    ap.add_argument("--uneven", action="store_true", help="also time the uneven-size 6-series group pass")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-size 6-series group pass")
+    ap.add_argument("--no-large", action="store_true", help="skip the 256^2-window (cluster) sample")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
