@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mset_b200.h"
 #include "mset_kernels.cuh"
 #include "mset_rotate.cuh"
@@ -30,8 +32,19 @@ int fail(int code, const char *fmt, ...) {
 }
 
 int cuda_fail(cudaError_t e, const char *where) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // not sticky: clear it so that later calls see a clean state
+        return fail(MSET_E_NOMEM, "%s: out of device memory", where);
+    }
     return fail(MSET_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
 }
+
+// NVTX range around an entry point (visible in Nsight timelines; no cost
+// without a tool attached)
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 #define CK(call)                                                    \
     do {                                                            \
@@ -257,6 +270,17 @@ int upload_tilt_measured(mset_session *s, TiltBufs &t, const float *meas) {
     const size_t n2 = (size_t)s->n * s->n;
     const size_t cnt = n2 * t.npos;
     if (cnt == 0) return 0;
+    // intensities are square-rooted in the loss: a negative, NaN or infinite
+    // count would turn every gradient of the pass into NaN
+    size_t bad = cnt;
+    for (size_t i = 0; i < cnt; ++i)
+        if (!(meas[i] >= 0.f) || meas[i] == INFINITY) {
+            bad = i;
+            break;
+        }
+    if (bad < cnt)
+        return fail(MSET_E_ARG, "measured pattern %zu has a negative, NaN or infinite value at pixel %zu (%g)",
+                    bad / n2, bad % n2, (double)meas[bad]);
     CK(s->meas_tmp.ensure(std::max(s->meas_tmp.n, cnt)));
     CK(cudaMemcpyAsync(s->meas_tmp.p, meas, sizeof(float) * cnt, cudaMemcpyHostToDevice, s->st));
     if (s->batch && s->amp_bf16) {
@@ -508,10 +532,12 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
 
 int mset_run(mset_session *s, int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out,
              float *error_out) {
+    Range range_("mset_run");
     return mset_run_ex(s, mode, MSET_ADJOINT_REF, rvol_out, probe_out, scan_x_out, scan_y_out, error_out);
 }
 
 int mset_error(mset_session *s, int mode, float *error_out) {
+    Range range_("mset_error");
     if (!s) return fail(MSET_E_ARG, "null session");
     int rc = check_mode(mode);
     if (rc) return rc;
@@ -683,6 +709,7 @@ static int batch_pass(mset_session *s) {
 }
 
 int mset_batch_gradient(mset_session *s, double *grad_out, double *probe_out, double *posdir_out, double *err_out) {
+    Range range_("mset_batch_gradient");
     int rc = batch_ok(s);
     if (rc) return rc;
     rc = batch_pass(s);
@@ -726,6 +753,7 @@ int mset_batch_read_gradient(mset_session *s, double *grad_out, double *probe_ou
 }
 
 int mset_batch_error(mset_session *s, double *err_out) {
+    Range range_("mset_batch_error");
     int rc = batch_ok(s);
     if (rc) return rc;
     CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * s->tilts.size(), s->st));
@@ -741,6 +769,7 @@ int mset_batch_error(mset_session *s, double *err_out) {
 }
 
 int mset_batch_simulate(mset_session *s, float *inten_out) {
+    Range range_("mset_batch_simulate");
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!inten_out) return fail(MSET_E_ARG, "null output");
@@ -825,6 +854,7 @@ static int rot_prepare(mset_session *s, int n) {
 
 int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int n, const float *vec1,
                        const float *vec2, const float *vec3, double phi, double theta, double psi, int inverse) {
+    Range range_("mset_rotate_volume");
     if (!s || !vol_in || !vol_out || !vec1 || !vec2 || !vec3) return fail(MSET_E_ARG, "null argument");
     if (n <= 1) return fail(MSET_E_ARG, "bad volume size %d", n);
     int rc = set_device(s);
@@ -846,6 +876,7 @@ int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int
 // ---- TV / TV-FISTA ----------------------------------------------------------
 int mset_tv(mset_session *s, float *vol, int n1, int n2, int n3, double lambda, int niter, int fista,
             double *tv_error) {
+    Range range_("mset_tv");
     if (!s || !vol) return fail(MSET_E_ARG, "null argument");
     if (n1 <= 0 || n2 <= 0 || n3 <= 0 || niter < 0 || !(lambda > 0))
         return fail(MSET_E_ARG, "need positive sizes, niter >= 0 and lambda > 0");
@@ -1031,6 +1062,7 @@ update:
 }
 
 int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_out, double *tv_err_out) {
+    Range range_("mset_batch_iterate");
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
@@ -1156,6 +1188,7 @@ static void drop_phase_graphs(mset_session *s) {
 
 int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, double *mean_err_out,
                            float *step_out, int *iters_out) {
+    Range range_("mset_batch_iterate_bls");
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
@@ -1225,6 +1258,7 @@ int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, dou
 }
 
 int mset_batch_iterate_phase(mset_session *s, int phase, int use_graph) {
+    Range range_("mset_batch_iterate_phase");
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
@@ -1563,6 +1597,7 @@ int group_launch(mset_group *g, const std::vector<int> &grids, bool use_graph) {
 extern "C" {
 
 int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out) {
+    Range range_("mset_batch_tune");
     int rc = batch_ok(s);
     if (rc) return rc;
     if (mem_budget_bytes < 0) return fail(MSET_E_ARG, "negative memory budget");
@@ -1674,6 +1709,7 @@ int mset_group_set_schedule(mset_group *g, int schedule) {
 }
 
 int mset_group_gradient(mset_group *g, int use_graph) {
+    Range range_("mset_group_gradient");
     if (!g) return fail(MSET_E_ARG, "null group");
     std::vector<int> grids;
     int rc = group_prepare(g, grids);
@@ -1705,6 +1741,7 @@ int mset_group_time(mset_group *g, int reps, int use_graph, double *ms_per_pass)
 }
 
 int mset_group_tune(mset_group *g, double mem_budget_bytes, int *schedule_out) {
+    Range range_("mset_group_tune");
     if (!g) return fail(MSET_E_ARG, "null group");
     if (g->m.empty()) return fail(MSET_E_STATE, "empty group");
     if (mem_budget_bytes < 0) return fail(MSET_E_ARG, "negative memory budget");

@@ -253,3 +253,35 @@ def test_gradient_without_measured_patterns_is_an_error(gpu_available):
     with pytest.raises(mset_b200.MsetError, match="measured patterns"):
         bs.gradient()
     bs.close()
+
+
+def test_invalid_measured_values_are_rejected(gpu_available):
+    """intensities are square-rooted: negative, NaN or infinite counts are
+    refused at upload with the pattern and pixel named"""
+    import mset_b200
+    c = small_case(n=24, nz=2, npos=3)
+    for bad in (-1.0, np.nan, np.inf):
+        meas = c["meas"].copy()
+        meas[1, 5, 7] = bad
+        with Session() as s:
+            with pytest.raises(mset_b200.MsetError, match="pattern 1 has a negative, NaN or infinite"):
+                s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"],
+                         scan_x=c["sx"], scan_y=c["sy"], measured=meas)
+        bs = BatchSession(n=24, nz=2, npos=[3], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+        with pytest.raises(mset_b200.MsetError, match="negative, NaN or infinite"):
+            bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=meas, volume=c["V"])
+        bs.close()
+
+
+def test_out_of_device_memory_is_reported_and_recoverable(gpu_available):
+    """a request beyond the device's memory fails with MSET_E_NOMEM (the
+    volume of 4e6 slices of 128^2 is 262 GB) and leaves the device usable"""
+    import mset_b200
+    c = small_case(n=128, nz=2, npos=2)
+    with pytest.raises(mset_b200.MsetError, match="out of device memory") as ei:
+        BatchSession(n=128, nz=4_000_000, npos=[1], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+    assert ei.value.code == -5
+    bs = BatchSession(n=128, nz=2, npos=[2], prop=c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"])
+    bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"], volume=c["V"])
+    assert np.isfinite(bs.gradient()["grad"]).all()
+    bs.close()
