@@ -224,8 +224,10 @@ def run_ours(args):
     # the plain form (reference semantics: one position after another, each
     # updating volume, probe and position; mset_run) and the reference's own
     # CUDA module (oracle/_ref, cuFFT) on a sample of the same tilt
-    plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (rank == 0 and not args.no_plain) else None
-    side = rank == 0 and args.config == "mid"
+    # side measurements: one GPU only (under torchrun the other ranks would
+    # wait for rank 0 in the next collective)
+    plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (world == 1 and not args.no_plain) else None
+    side = world == 1 and args.config == "mid"
     uneven = uneven_batch(args, local) if (side and not args.no_uneven) else None
     large = large_window(args, local) if (side and not args.no_large) else None
 
