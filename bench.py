@@ -256,7 +256,7 @@ def run_ours(args):
         fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, FMA counted as 2
         flop = units * flops_per_unit(n) + positions * flops_per_position(n)
         achieved = flop / (ms / 1e3) / 1e12
-        cpu = cpu_baseline(args, cfg, spec, meas) if not args.no_cpu else None
+        cpu = cpu_baseline(args, cfg, spec, meas) if (not args.no_cpu and world == 1) else None
         line = {
             "metric": "slice-propagations/s (fwd+adjoint)",
             "value": value,
