@@ -232,9 +232,19 @@ def run_ours(args):
     large = large_window(args, local) if (side and not args.no_large) else None
 
     # end to end through the C ABI with host buffers: volumes in, gradients out
-    vols = [np.ascontiguousarray(0.5 * v) for v in spec.volumes]
-    grad = np.zeros((cfg.n_tilts, ns, n, n))
-    err = np.zeros(cfg.n_tilts)
+    # host buffers in pinned (page-locked) memory, as a production caller
+    # would keep its per-step inputs and outputs
+    def pinned(shape, dtype):
+        t = torch.empty(shape, dtype=dtype, pin_memory=True)
+        return t.numpy()
+
+    vols = []
+    for v in spec.volumes:
+        hv = pinned(v.shape, torch.float32)
+        hv[...] = 0.5 * v
+        vols.append(hv)
+    grad = pinned((cfg.n_tilts, ns, n, n), torch.float64)
+    err = pinned((cfg.n_tilts,), torch.float64)
     import ctypes as C
     from mset_b200._lib import check, dptr, fptr
     e2e_steps = max(1, min(args.steps, 3))
@@ -290,7 +300,7 @@ def run_ours(args):
                          "peak_source": f"nominal FP32 CUDA-core peak 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz "
                                         "(MEASURED_PEAKS has no FP32 figure)",
                          "flop_per_unit": flops_per_unit(n), "flop_per_position": flops_per_position(n)},
-            "e2e": {"value": world * units / e2e_s, "unit": "slice-propagations/s",
+            "e2e": {"value": world * units / e2e_s, "unit": "slice-propagations/s", "host_memory": "pinned",
                     "h2d_bytes_per_step": int(sum(v.nbytes for v in vols)),
                     "d2h_bytes_per_step": int(grad.nbytes + err.nbytes)},
             "iteration": None if it_ms is None else {
