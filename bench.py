@@ -300,6 +300,16 @@ def run_ours(args):
                          "peak_source": f"nominal FP32 CUDA-core peak 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz "
                                         "(MEASURED_PEAKS has no FP32 figure)",
                          "flop_per_unit": flops_per_unit(n), "flop_per_position": flops_per_position(n)},
+            # the same kernel against the measured HBM copy rate (it is not
+            # HBM-bound: FP32 issue and the shared-memory data path bound it)
+            "roofline_hbm": {"bound": "hbm", "unit": "GB/s",
+                             "achieved": units * (16 * n * n + 4 * n * n / ns) / (ms / 1e3) / 1e9,
+                             "peak": float(peaks.get("hbm_gbs", 6650.0)),
+                             "frac": units * (16 * n * n + 4 * n * n / ns) / (ms / 1e3) / 1e9
+                             / float(peaks.get("hbm_gbs", 6650.0)),
+                             "traffic": TRAFFIC_PER_UNIT * units * (n / 128.0) ** 2,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
+                             else "fallback 6.65 TB/s"},
             "e2e": {"value": world * units / e2e_s, "unit": "slice-propagations/s", "host_memory": "pinned",
                     "h2d_bytes_per_step": int(sum(v.nbytes for v in vols)),
                     "d2h_bytes_per_step": int(grad.nbytes + err.nbytes)},
