@@ -185,7 +185,9 @@ int mset_batch_read_gradient(mset_session *s, double *grad, double *probe, doubl
  * shape).  Times the batched pass on a sample of the session's own positions
  * (up to 4 x SMs x resident CTAs) for every shape whose saved-wave storage fits
  * mem_budget_bytes (0: no limit) and keeps the fastest, or among shapes within
- * 1% of it the one using less memory.  Shape = persistent CTAs (SMs x CTAs per
+ * 1% of it the one using less memory.  Shape = kernel thread shape (for
+ * 64, 96, 128 and 160 two compiled shapes: threads per CTA and the register
+ * budget that goes with them) x persistent CTAs (SMs x CTAs per
  * SM, i.e. positions in flight) x checkpoint interval k in {0, 2, 4, 8, 16}
  * (k < slabs; k = 0 keeps every wave).  The choice stays with the session
  * (mset_batch_set_checkpoint overrides k).  MSET_E_NOMEM when no shape fits. */
@@ -196,8 +198,15 @@ typedef struct {
     int32_t candidates;     /* shapes timed */
     double us_per_position; /* measured device time per position at this shape */
     double save_bytes;      /* saved-wave storage at this shape */
+    int32_t threads;        /* threads per CTA of the chosen kernel shape */
+    int32_t reserved;
 } mset_tune_result;
 int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out);
+/* compiled kernel shapes of window size n (threads per CTA and register
+ * budget; same results), and the choice of one for a session (0: default;
+ * resets the tuned batch shape) */
+int mset_batch_variants(int n);
+int mset_batch_set_variant(mset_session *s, int variant);
 /* the shape the next batched pass uses (candidates = 0; us_per_position = 0
  * when the session was not tuned) */
 int mset_batch_get_tune(mset_session *s, mset_tune_result *out);

@@ -67,6 +67,8 @@ SIGNATURES = {
     "mset_batch_read_gradient": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
     "mset_batch_tune": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "mset_batch_get_tune": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mset_batch_variants": (C.c_int, [C.c_int]),
+    "mset_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_group_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "mset_group_destroy": (C.c_int, [C.c_void_p]),
     "mset_group_add": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -149,6 +151,8 @@ class TuneResult(C.Structure):
         ("candidates", C.c_int32),
         ("us_per_position", C.c_double),
         ("save_bytes", C.c_double),
+        ("threads", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
     def as_dict(self):

@@ -93,6 +93,13 @@ class BatchSession:
         check("mset_batch_tune", self._lib.mset_batch_tune(self._h, float(mem_budget_bytes), C.byref(r)))
         return r.as_dict()
 
+    def set_variant(self, variant: int):
+        """use compiled kernel shape `variant` of this window (mset_batch_set_variant)"""
+        check("mset_batch_set_variant", self._lib.mset_batch_set_variant(self._h, int(variant)))
+
+    def variants(self) -> int:
+        return int(self._lib.mset_batch_variants(self.n))
+
     def shape(self) -> dict:
         """the batch shape the next pass uses (mset_batch_get_tune)"""
         r = _lib.TuneResult()

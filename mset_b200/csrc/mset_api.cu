@@ -1397,19 +1397,38 @@ int time_queue(mset_session *s, int grid, int nitems, int reps, double *ms) {
 }
 
 int tune_session(mset_session *s, double budget, mset_tune_result *out) {
-    const int occ = occupancy_limit(s);
     std::vector<int> ks{0};
     if (s->method == MSET_MODE_MSET)
         for (int k : {2, 4, 8, 16})
             if (k < s->ns) ks.push_back(k);
     const int k_in = s->ckpt;
-    const int sample = std::min(s->total_pos, 4 * s->sms * occ);
+    const Plan plan_in = s->plan;
+    // the same positions for every shape: as many as the widest grid of any
+    // variant keeps busy four times over
+    int occ_max = 1;
+    for (int v = 0; v < plan_variants(s->n); ++v) {
+        Plan pl;
+        if (plan_for(s->n, &pl, v)) {
+            s->plan = pl;
+            occ_max = std::max(occ_max, occupancy_limit(s));
+        }
+    }
+    s->plan = plan_in;
+    const int sample = std::min(s->total_pos, 4 * s->sms * occ_max);
     int rc = batch_zero(s);
     if (!rc) rc = batch_transmission(s);
     if (rc) return rc;
-    int best_grid = 0, best_k = 0, timed = 0, last_grid = 0;
+    int best_grid = 0, best_k = 0, timed = 0;
     double best_us = 0, best_bytes = 0;
+    Plan best_plan = plan_in;
     const int tuned_in = s->tuned_grid;
+    for (int v = 0; v < plan_variants(s->n); ++v) {
+    Plan pl;
+    if (!plan_for(s->n, &pl, v)) continue;
+    pl.max_clusters = plan_in.max_clusters;
+    s->plan = pl;
+    const int occ = occupancy_limit(s);
+    int last_grid = 0;
     for (int c = 1; c <= occ; ++c) {
         s->tuned_grid = 0;
         const int grid = s->plan.cl > 1 ? persistent_grid(s, s->total_pos)
@@ -1425,6 +1444,7 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
             rc = time_queue(s, grid, sample, 2, &ms);
             if (rc) {
                 s->ckpt = k_in;
+                s->plan = plan_in;
                 return rc;
             }
             ++timed;
@@ -1436,10 +1456,14 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
                 best_grid = grid;
                 best_k = k;
                 best_bytes = bytes;
+                best_plan = s->plan;
             }
         }
     }
+    }
+    s->plan = best_plan;
     if (!best_grid) {
+        s->plan = plan_in;
         s->ckpt = k_in;
         return fail(MSET_E_NOMEM, "no batch shape of the %d^2 window fits the memory budget of %.0f bytes", s->n,
                     budget);
@@ -1462,6 +1486,7 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
         out->candidates = timed;
         out->us_per_position = best_us;
         out->save_bytes = best_bytes;
+        out->threads = s->plan.nt;
     }
     return 0;
 }
@@ -1557,6 +1582,7 @@ int group_prepare(mset_group *g, std::vector<int> &grids) {
                               (const void *)s->counter.p, (const void *)s->err.p})
             sig.push_back(p);
         sig.push_back(reinterpret_cast<const void *>((intptr_t)grids[i]));
+        sig.push_back(s->plan.ops);
         sig.push_back(reinterpret_cast<const void *>((intptr_t)s->ckpt));
         sig.push_back(reinterpret_cast<const void *>((intptr_t)s->total_pos));
         for (const TiltBufs &t : s->tilts) {
@@ -1605,6 +1631,23 @@ int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *
     return tune_session(s, mem_budget_bytes, out);
 }
 
+int mset_batch_variants(int n) { return plan_variants(n); }
+
+int mset_batch_set_variant(mset_session *s, int variant) {
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    Plan pl;
+    if (variant < 0 || !plan_for(s->n, &pl, variant))
+        return fail(MSET_E_ARG, "window %d has %d kernel shapes, not %d", s->n, plan_variants(s->n), variant + 1);
+    pl.max_clusters = s->plan.max_clusters;
+    s->plan = pl;
+    s->tuned_grid = 0;
+    s->tuned_us_per_pos = 0;
+    s->grid_cache = 0;
+    drop_graph(s);
+    return 0;
+}
+
 int mset_batch_get_tune(mset_session *s, mset_tune_result *out) {
     int rc = batch_ok(s);
     if (rc) return rc;
@@ -1616,6 +1659,7 @@ int mset_batch_get_tune(mset_session *s, mset_tune_result *out) {
     out->candidates = 0;
     out->us_per_position = s->tuned_us_per_pos;
     out->save_bytes = save_bytes(s, grid, s->ckpt);
+    out->threads = s->plan.nt;
     return 0;
 }
 

@@ -6,21 +6,33 @@
 
 namespace mset {
 
-#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(96) X(128) X(160) X(256)
+// every compiled geometry; the first entry of a window size is its default,
+// the others are alternative thread shapes the autotuner may pick
+#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(64v2) X(96) X(96v2) X(128) X(128v2) X(160) X(160v2) X(256)
 #define X(N_) extern const GeoOps kGeo##N_;
 MSET_GEOS(X)
 #undef X
 
-static const GeoOps *find_geo(int n) {
-#define X(N_) \
-    if (n == N_) return &kGeo##N_;
+static const GeoOps *const kAllGeos[] = {
+#define X(N_) &kGeo##N_,
     MSET_GEOS(X)
 #undef X
+};
+
+static const GeoOps *find_geo(int n, int variant) {
+    for (const GeoOps *g : kAllGeos)
+        if (g->n == n && variant-- == 0) return g;
     return nullptr;
 }
 
-bool plan_for(int n, Plan *p) {
-    const GeoOps *g = find_geo(n);
+int plan_variants(int n) {
+    int c = 0;
+    for (const GeoOps *g : kAllGeos) c += g->n == n;
+    return c;
+}
+
+bool plan_for(int n, Plan *p, int variant) {
+    const GeoOps *g = find_geo(n, variant);
     if (!g) return false;
     p->n = g->n;
     p->r1 = g->r1;

@@ -82,7 +82,9 @@ struct Plan {
     int ctas_per_sm;
     const GeoOps *ops;
 };
-bool plan_for(int n, Plan *p);
+// geometry `variant` (0: default) of window size n; plan_variants(n) of them exist
+bool plan_for(int n, Plan *p, int variant = 0);
+int plan_variants(int n);
 int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,
                      cudaStream_t st);
 int launch_prep_amp(const Plan &pl, const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);

@@ -805,22 +805,26 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
 }  // namespace mset
 
 // one translation unit per window size defines its table entry
-#define MSET_DEFINE_GEO(N_, R1_, NT_, MINB_) MSET_DEFINE_GEO_T(N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
+#define MSET_DEFINE_GEO(N_, R1_, NT_, MINB_) MSET_DEFINE_GEO_T(N_, N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
+// another thread / register shape of the same window (same R1, so the same
+// scrambled layouts): a choice for the autotuner, table entry kGeo<NAME_>
+#define MSET_DEFINE_GEO_VARIANT(NAME_, N_, R1_, NT_, MINB_) \
+    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
 // a field split by rows over a cluster of CL_ CTAs
-#define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
+#define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
 #define MSET_UNPAREN(...) __VA_ARGS__
-#define MSET_DEFINE_GEO_T(N_, R1_, GT_)                                                \
+#define MSET_DEFINE_GEO_T(NAME_, N_, R1_, GT_)                                         \
     namespace mset {                                                                   \
-    using Geo##N_ = MSET_UNPAREN GT_;                                                  \
-    extern const GeoOps kGeo##N_ = {N_,                                                \
-                                    R1_,                                               \
-                                    Geo##N_::NT,                                       \
-                                    Geo##N_::CL,                                       \
-                                    smem_bytes<Geo##N_>(),                             \
-                                    &geo_max_clusters<Geo##N_>,                        \
-                                    &geo_positions<Geo##N_>,                           \
-                                    &geo_prep_amp<Geo##N_>,                            \
-                                    &geo_prep_amp_bf16<Geo##N_>,                       \
-                                    &geo_prep_prop<Geo##N_>,                           \
-                                    &geo_probe_q<Geo##N_>};                            \
+    using Geo##NAME_ = MSET_UNPAREN GT_;                                               \
+    extern const GeoOps kGeo##NAME_ = {N_,                                             \
+                                       R1_,                                            \
+                                       Geo##NAME_::NT,                                 \
+                                       Geo##NAME_::CL,                                 \
+                                       smem_bytes<Geo##NAME_>(),                       \
+                                       &geo_max_clusters<Geo##NAME_>,                  \
+                                       &geo_positions<Geo##NAME_>,                     \
+                                       &geo_prep_amp<Geo##NAME_>,                      \
+                                       &geo_prep_amp_bf16<Geo##NAME_>,                 \
+                                       &geo_prep_prop<Geo##NAME_>,                     \
+                                       &geo_probe_q<Geo##NAME_>};                      \
     }

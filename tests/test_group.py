@@ -156,3 +156,29 @@ def test_group_rejects_a_repeated_member(gpu_available):
         mset_b200._lib.check("mset_group_add", grp._lib.mset_group_add(grp._h, bs._h))
     grp.close()
     bs.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [64, 96, 128, 160])
+def test_every_kernel_shape_matches_default_and_oracle(gpu_available, n):
+    """the alternative thread shapes of a window (the autotuner's choices)
+    give the default shape's results and the oracle's"""
+    from oracle import oracle as O
+    spec = dict(n=n, nz=4, b=1, npos=3, tilts=1, adjoint=MSET_ADJOINT_REF)
+    bs, tilts = _series(spec, 1000 + n)
+    assert bs.variants() == 2
+    outs = []
+    for v in range(bs.variants()):
+        bs.set_variant(v)
+        outs.append(bs.gradient())
+        assert bs.shape()["threads"] > 0
+    with pytest.raises(mset_b200.MsetError, match="kernel shapes"):
+        bs.set_variant(2)
+    bs.close()
+    _same(outs[1], outs[0])
+    c = tilts[0]
+    g, pa, pd, e = O.batched_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"], sigma=c["sigma"],
+                                  dz=c["dz"], binning=1)
+    assert rel_l2(outs[1]["grad"][0], g) < TOL
+    assert rel_l2(np.fft.fft2(outs[1]["probe"][0]), pa) < TOL
+    assert abs(outs[1]["err"][0] - e) <= TOL * e
