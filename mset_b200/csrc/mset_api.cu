@@ -1423,43 +1423,43 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
     Plan best_plan = plan_in;
     const int tuned_in = s->tuned_grid;
     for (int v = 0; v < plan_variants(s->n); ++v) {
-    Plan pl;
-    if (!plan_for(s->n, &pl, v)) continue;
-    pl.max_clusters = plan_in.max_clusters;
-    s->plan = pl;
-    const int occ = occupancy_limit(s);
-    int last_grid = 0;
-    for (int c = 1; c <= occ; ++c) {
-        s->tuned_grid = 0;
-        const int grid = s->plan.cl > 1 ? persistent_grid(s, s->total_pos)
-                                        : std::max(1, std::min(s->sms * c, s->total_pos));
-        s->tuned_grid = tuned_in;
-        if (grid == last_grid) break;
-        last_grid = grid;
-        for (int k : ks) {
-            const double bytes = save_bytes(s, grid, k);
-            if (budget > 0 && bytes > budget) continue;
-            s->ckpt = k;
-            double ms = 0;
-            rc = time_queue(s, grid, sample, 2, &ms);
-            if (rc) {
-                s->ckpt = k_in;
-                s->plan = plan_in;
-                return rc;
-            }
-            ++timed;
-            const double us = ms * 1e3 / sample;
-            const bool faster = !best_grid || us < 0.99 * best_us;
-            const bool tie_smaller = best_grid && us <= 1.01 * best_us && bytes < best_bytes;
-            if (faster || tie_smaller) {
-                if (faster || us < best_us) best_us = us;
-                best_grid = grid;
-                best_k = k;
-                best_bytes = bytes;
-                best_plan = s->plan;
+        Plan pl;
+        if (!plan_for(s->n, &pl, v)) continue;
+        pl.max_clusters = plan_in.max_clusters;
+        s->plan = pl;
+        const int occ = occupancy_limit(s);
+        int last_grid = 0;
+        for (int c = 1; c <= occ; ++c) {
+            s->tuned_grid = 0;
+            const int grid = s->plan.cl > 1 ? persistent_grid(s, s->total_pos)
+                                            : std::max(1, std::min(s->sms * c, s->total_pos));
+            s->tuned_grid = tuned_in;
+            if (grid == last_grid) break;
+            last_grid = grid;
+            for (int k : ks) {
+                const double bytes = save_bytes(s, grid, k);
+                if (budget > 0 && bytes > budget) continue;
+                s->ckpt = k;
+                double ms = 0;
+                rc = time_queue(s, grid, sample, 2, &ms);
+                if (rc) {
+                    s->ckpt = k_in;
+                    s->plan = plan_in;
+                    return rc;
+                }
+                ++timed;
+                const double us = ms * 1e3 / sample;
+                const bool faster = !best_grid || us < 0.99 * best_us;
+                const bool tie_smaller = best_grid && us <= 1.01 * best_us && bytes < best_bytes;
+                if (faster || tie_smaller) {
+                    if (faster || us < best_us) best_us = us;
+                    best_grid = grid;
+                    best_k = k;
+                    best_bytes = bytes;
+                    best_plan = s->plan;
+                }
             }
         }
-    }
     }
     s->plan = best_plan;
     if (!best_grid) {
