@@ -303,7 +303,8 @@ int mset_batch_device_info(mset_session *s, void **gacc_dev, size_t *gacc_count,
  * degrees, split into sub-rotations of at most 11 degrees of four Fourier
  * shears each.  vol_in / vol_out: host [n][n][n] float (MATLAB n x n x n),
  * may alias.  All angles within 0.5 degrees: copied unchanged, as the
- * reference does.  Cubic volumes with n in {24, 32, 48, 64, 96, 128, 160}. */
+ * reference does.  Cubic volumes with n in {24, 32, 48, 64, 96, 128, 160, 256}
+ * (256: each plane split over a 4-CTA thread-block cluster). */
 int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int n, const float *vec1,
                        const float *vec2, const float *vec3, double phi, double theta, double psi, int inverse);
 

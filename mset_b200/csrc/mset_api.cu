@@ -837,7 +837,7 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
 static int rot_prepare(mset_session *s, int n) {
     if (!rot_supported(n))
         return fail(MSET_E_UNSUPPORTED, "rotation of a %d^3 volume has no compiled kernel "
-                                        "(supported: 24, 32, 48, 64, 96, 128, 160)", n);
+                                        "(supported: 24, 32, 48, 64, 96, 128, 160, 256)", n);
     const size_t n3 = (size_t)n * n * n;
     CK(s->rot_vol.ensure(n3));
     CK(s->rot_S.ensure(n3));

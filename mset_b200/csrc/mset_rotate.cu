@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
     constexpr int N = G::N, R1 = G::R1, R2 = G::R2;
     extern __shared__ __align__(16) float2 sm[];
     float2 *buf = sm;
-    float2 *tw = buf + N * G::S;
+    float2 *tw = buf + G::FIELD;
     float2 *ex = tw + N;
     float2 *ey = ex + N;
     __shared__ int nyx[N], nyy[N];
@@ -81,19 +81,22 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
         sx = 1; sy = N; sc = nn;      // plane (i1, i2) at fixed i3
     }
     const float inv = 1.0f / (float)(N * N);
-    for (int c = blockIdx.x; c < N; c += gridDim.x) {
+    // one plane per CTA, or per cluster when the plane is split by rows
+    const int y_lo = G::row0();
+    sync_all<G>();  // (cluster) every CTA has started before any remote access
+    for (int c = blockIdx.x / G::CL; c < N; c += gridDim.x / G::CL) {
         bool qc;
         const int gc = rot_grid_val(c, N, &qc);
         if (qc) {
             // the reference's grids are zero on this plane: no shift; only the
             // fourth shear's real() acts
             if (REAL) {
-                for (int i = threadIdx.x; i < N * N; i += G::NT) {
-                    float2 *p = S + (long)c * sc + (long)(i / N) * sy + (long)(i % N) * sx;
+                for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
+                    float2 *p = S + (long)c * sc + (long)(y_lo + i / N) * sy + (long)(i % N) * sx;
                     p->y = 0.f;
                 }
             }
-            __syncthreads();
+            sync_all<G>();
             continue;
         }
         // per-plane phase factors (double): phase = 2 pi gc (cx gx(kx) + cy gy(ky)) / N
@@ -117,15 +120,15 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
             ey[L] = make_float2((float)co, (float)s);
             nyy[L] = q;
         }
-        for (int i = threadIdx.x; i < N * N; i += G::NT) {
+        for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
             const int yy = i / N, xx = i % N;
-            buf[G::at(yy, xx)] = S[(long)c * sc + (long)yy * sy + (long)xx * sx];
+            buf[G::at(yy, xx)] = S[(long)c * sc + (long)(y_lo + yy) * sy + (long)xx * sx];
         }
         __syncthreads();
         row_passA<G, 0, -1>(buf, tw, NoOp{});
         sync_rows();
         row_passB<G, -1>(buf);
-        sync_all();
+        sync_all<G>();
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
         col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -139,54 +142,72 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
         });
         sync_cols<G>();
         col_passA<G, +1, false>(buf, tw);
-        sync_all();
+        sync_all<G>();
         row_passB<G, +1>(buf);
         sync_rows();
         row_passA<G, +1, 0>(buf, tw, NoOp{});
         __syncthreads();
-        for (int i = threadIdx.x; i < N * N; i += G::NT) {
+        for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
             const int yy = i / N, xx = i % N;
             float2 v = buf[G::at(yy, xx)];
             if (REAL) v.y = 0.f;
-            S[(long)c * sc + (long)yy * sy + (long)xx * sx] = v;
+            S[(long)c * sc + (long)(y_lo + yy) * sy + (long)xx * sx] = v;
         }
-        __syncthreads();
+        sync_all<G>();
         (void)R2;
     }
 }
 
 template <class G>
 static size_t shear_smem() {
-    return sizeof(float2) * ((size_t)G::N * G::S + 3 * G::N);
+    return sizeof(float2) * ((size_t)G::FIELD + 3 * G::N);
+}
+
+template <class G, bool REAL>
+static int launch_shear_k(float2 *S, const float2 *twn, int dim, double a, double b, int grid, cudaStream_t st) {
+    auto k = k_shear<G, REAL>;
+    const size_t sm = shear_smem<G>();
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return (int)e;
+    if constexpr (G::CL > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(G::NT);
+        cfg.dynamicSmemBytes = sm;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = G::CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return (int)cudaLaunchKernelEx(&cfg, k, S, twn, dim, a, b);
+    } else {
+        k<<<grid, G::NT, sm, st>>>(S, twn, dim, a, b);
+        return (int)cudaGetLastError();
+    }
 }
 
 template <class G>
 static int launch_shear(float2 *S, const float2 *twn, int dim, double a, double b, bool real, int sms,
                         cudaStream_t st) {
-    const size_t sm = shear_smem<G>();
-    const int grid = std::min(G::N, sms);
-    if (real) {
-        auto k = k_shear<G, true>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return (int)e;
-        k<<<grid, G::NT, sm, st>>>(S, twn, dim, a, b);
-    } else {
-        auto k = k_shear<G, false>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return (int)e;
-        k<<<grid, G::NT, sm, st>>>(S, twn, dim, a, b);
-    }
-    return (int)cudaGetLastError();
+    // planes in flight: one per CTA, or one per cluster of CL CTAs
+    const int grid = std::min(G::N, sms / G::CL) * G::CL;
+    return real ? launch_shear_k<G, true>(S, twn, dim, a, b, grid, st)
+                : launch_shear_k<G, false>(S, twn, dim, a, b, grid, st);
 }
 
 #define MSET_ROT_GEOS(X) X(24, 8, 64) X(32, 8, 128) X(48, 16, 192) X(64, 8, 256) X(96, 16, 384) X(128, 16, 512) X(160, 16, 640)
+// 256^2 planes do not fit one SM: split by rows over a 4-CTA cluster
+using RotGeo256 = GeoCl<256, 16, 512, 4>;
 
 bool rot_supported(int n) {
 #define X(N_, R1_, NT_) \
     if (n == N_) return true;
     MSET_ROT_GEOS(X)
 #undef X
-    return false;
+    return n == 256;
 }
 
 int rot_r1(int n) {
@@ -194,7 +215,7 @@ int rot_r1(int n) {
     if (n == N_) return R1_;
     MSET_ROT_GEOS(X)
 #undef X
-    return 0;
+    return n == 256 ? RotGeo256::R1 : 0;
 }
 
 static int shear(int n, float2 *S, const float2 *twn, int dim, double a, double b, bool real, int sms,
@@ -203,6 +224,7 @@ static int shear(int n, float2 *S, const float2 *twn, int dim, double a, double 
     if (n == N_) return launch_shear<Geo<N_, R1_, NT_>>(S, twn, dim, a, b, real, sms, st);
     MSET_ROT_GEOS(X)
 #undef X
+    if (n == 256) return launch_shear<RotGeo256>(S, twn, dim, a, b, real, sms, st);
     return (int)cudaErrorInvalidValue;
 }
 

@@ -75,3 +75,21 @@ def test_gpu_rotation_matches_oracle(gpu_available, n, angles, inverse):
                                                                fptr(vecs[1]), fptr(vecs[2]), float(angles[0]),
                                                                float(angles[1]), float(angles[2]), inverse))
     assert rel_l2(out, ref) < 1e-4
+
+
+@pytest.mark.gpu
+def test_gpu_rotation_256_cluster_matches_oracle_samples(gpu_available):
+    """256^3: every plane split over a 4-CTA cluster; checked on 8,192 seeded
+    voxels of the FP64 oracle's result (tests/golden/make_rot256_fixture.py)"""
+    import os
+
+    from mset_b200 import Session
+    from tests.golden.make_rot256_fixture import volume
+
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", "rot256.npz"))
+    v = volume()
+    with Session() as s:
+        for i in range(2):
+            out = s.rotate_volume(v, f[f"angles{i}"], inverse=bool(f[f"inverse{i}"]))
+            vals = out.reshape(-1)[f["idx"]]
+            assert rel_l2(vals, f[f"values{i}"]) < 1e-4
