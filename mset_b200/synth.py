@@ -63,6 +63,9 @@ CONFIGS = {
     "large": Config("large", (192, 256, 256), 0.25, 256, (64, 64), 4.0, 41, 70.0, 2, 1e4),
     # its geometry on 3 of the tilts (-70, 0, +70 deg), for timing samples
     "large_s": Config("large_s", (192, 256, 256), 0.25, 256, (64, 64), 4.0, 3, 70.0, 2, 1e4),
+    # a cubic 256^3 reconstruction in the same window (the batched iteration
+    # rotates cubic volumes), 128 slices of 2 voxels, on 3 tilts
+    "large_cubic_s": Config("large_cubic_s", (256, 256, 256), 0.25, 256, (64, 64), 4.0, 3, 70.0, 2, 1e4),
     # its geometry on 1 tilt x 12x12 positions, for profiling captures
     "large_p": Config("large_p", (192, 256, 256), 0.25, 256, (12, 12), 4.0, 1, 0.0, 2, 1e4),
 }
