@@ -166,16 +166,17 @@ def test_every_kernel_shape_matches_default_and_oracle(gpu_available, n):
     from oracle import oracle as O
     spec = dict(n=n, nz=4, b=1, npos=3, tilts=1, adjoint=MSET_ADJOINT_REF)
     bs, tilts = _series(spec, 1000 + n)
-    assert bs.variants() == 2
+    assert bs.variants() >= 2
     outs = []
     for v in range(bs.variants()):
         bs.set_variant(v)
         outs.append(bs.gradient())
         assert bs.shape()["threads"] > 0
     with pytest.raises(mset_b200.MsetError, match="kernel shapes"):
-        bs.set_variant(2)
+        bs.set_variant(len(outs))
     bs.close()
-    _same(outs[1], outs[0])
+    for o in outs[1:]:
+        _same(o, outs[0])
     c = tilts[0]
     g, pa, pd, e = O.batched_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"], sigma=c["sigma"],
                                   dz=c["dz"], binning=1)
