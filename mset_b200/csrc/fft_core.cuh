@@ -261,31 +261,38 @@ struct Geo {
     // scrambled location -> frequency index
     __host__ __device__ __forceinline__ static int scr(int L) { return L / R1 + R2 * (L % R1); }
     __device__ __forceinline__ static int rank() { return 0; }
-    __device__ __forceinline__ static int row0() { return 0; }
+    // row of the field held at local row l (yb = ybase(), read once per pass)
+    __device__ __forceinline__ static int ybase() { return 0; }
+    __device__ __forceinline__ static int gy(int, int l) { return l; }
 };
 
 // A field too large for one SM's shared memory, split by rows over a
-// thread-block cluster of CL CTAs: CTA r holds rows [r*ROWS, (r+1)*ROWS) with
-// the same padded stride.  Row passes stay CTA-local.  A column transform
-// keeps the single-CTA factorisation N = R1*R2: its pass A (R2 points at rows
-// n1 + R1*j) reads and writes every CTA of the cluster through distributed
-// shared memory, each task owned by one thread so that the pass is in place;
-// its pass B (R1 consecutive rows j + R1*k2) is CTA-local because R1 divides
-// ROWS.  The scrambled layout is therefore the single-CTA one.
+// thread-block cluster of CL CTAs.  The column transform keeps the single-CTA
+// factorisation N = R1*R2 (so the scrambled layout is the single-CTA one),
+// and the rows are dealt out by their residue n1 = y mod R1: CTA r holds the
+// N1C = R1/CL residues [r*N1C, (r+1)*N1C), row y = n1 + R1*j at local row
+// (n1 - r*N1C)*R2 + j.  Row passes and column pass A (R2 points at rows
+// n1 + R1*j, one residue) are then CTA-local; only column pass B (R1 points
+// at rows j + R1*k2, one of every residue) reads and writes every CTA of the
+// cluster through distributed shared memory, each task owned by one thread so
+// that the pass is in place.  One distributed pass per column transform, and
+// the switch between row passes and column pass A needs only a CTA barrier.
 template <int N_, int R1_, int NT_, int CL_>
 struct GeoCl : Geo<N_, R1_, NT_, 1> {
     using Base = Geo<N_, R1_, NT_, 1>;
     static constexpr int CL = CL_;
     static constexpr int ROWS = N_ / CL_;
+    static constexpr int N1C = R1_ / CL_;  // residues n1 per CTA
     static constexpr int FIELD = ROWS * Base::S;
-    static_assert(N_ % CL_ == 0 && ROWS % R1_ == 0, "R1 must divide the rows of one CTA");
-    static_assert(Base::R2 % CL_ == 0 && R1_ % CL_ == 0, "column passes must split over the cluster");
+    static_assert(R1_ % CL_ == 0 && Base::R2 % CL_ == 0, "column passes must split over the cluster");
+    static_assert(N1C * Base::R2 == ROWS, "every CTA holds N1C whole residues");
     __device__ __forceinline__ static int rank() {
         unsigned r;
         asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
         return (int)r;
     }
-    __device__ __forceinline__ static int row0() { return rank() * ROWS; }
+    __device__ __forceinline__ static int ybase() { return rank() * N1C; }
+    __device__ __forceinline__ static int gy(int yb, int l) { return yb + l / Base::R2 + R1_ * (l % Base::R2); }
 };
 
 // twiddle W_N^{n1 k2} with sign (table holds e^{-2 pi i m/N} as [k2][n1])
@@ -320,17 +327,20 @@ __device__ __forceinline__ void sync_rows() { __syncwarp(); }
 __device__ __forceinline__ void cluster_sync() {
     asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
+// between column pass A and column pass B
 template <class G>
 __device__ __forceinline__ void sync_cols() {
     if constexpr (G::CL > 1) {
-        // the passes on either side touch rows of other CTAs
+        // column pass B touches rows of other CTAs
         cluster_sync();
     } else {
         // named barrier per warp pair (ids 1..15; 0 is __syncthreads)
         asm volatile("bar.sync %0, 64;" ::"r"(1 + Own<G>::pair()) : "memory");
     }
 }
-// switch between row and column passes (or any CTA-wide exchange)
+// switch between row passes and column pass A: CTA-local in both geometries
+__device__ __forceinline__ void sync_rowcol() { __syncthreads(); }
+// every thread of the field (the cluster when it is split)
 template <class G>
 __device__ __forceinline__ void sync_all() {
     if constexpr (G::CL > 1) cluster_sync();
@@ -375,17 +385,17 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
     constexpr int R1 = G::R1, R2 = G::R2;
     constexpr int TASKS = O::RPW * R1;
     const int yl0 = O::warp() * O::RPW;  // first local row of the warp
-    const int y0 = G::row0() + yl0;      // its row in the field (pf / op)
+    const int yb = G::ybase();           // local row -> row of the field (pf / op)
     // Pre::kAhead: issue the next task's global loads while the current task
     // runs (double-buffered prefetch); otherwise just before its shared reads
     constexpr bool ahead = Pre::kAhead;
     Pre pre, nxt;
-    if (ahead && O::lane() < TASKS) pf(y0 + O::lane() / R1, O::lane() % R1, pre);
+    if (ahead && O::lane() < TASKS) pf(G::gy(yb, yl0 + O::lane() / R1), O::lane() % R1, pre);
 #pragma unroll 1
     for (int tau = O::lane(); tau < TASKS; tau += 32) {
-        const int n1 = tau % R1, y = y0 + tau / R1;
+        const int n1 = tau % R1, y = G::gy(yb, yl0 + tau / R1);
         if constexpr (ahead) {
-            if (tau + 32 < TASKS) pf(y0 + (tau + 32) / R1, (tau + 32) % R1, nxt);
+            if (tau + 32 < TASKS) pf(G::gy(yb, yl0 + (tau + 32) / R1), (tau + 32) % R1, nxt);
         } else {
             pf(y, n1, pre);
         }
@@ -443,24 +453,17 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
     if constexpr (G::CL > 1) {
-        // distributed: CTA r owns the tasks n1 in [r*R1/CL, (r+1)*R1/CL) of
-        // every column; element j (row n1 + R1*j) lives in CTA j / JPC at
-        // local row n1 + R1*(j % JPC)
-        constexpr int JPC = R2 / G::CL;  // elements per CTA
-        constexpr int N1C = R1 / G::CL;  // n1 values per CTA
-        constexpr int TASKS = N1C * G::N;
-        uint32_t pb[G::CL];  // shared::cluster addresses of the CTAs' fields
-#pragma unroll
-        for (int r = 0; r < G::CL; ++r) pb[r] = peer_addr(buf, r);
-        const int n1b = G::rank() * N1C;
-        constexpr uint32_t kRow = sizeof(float2) * R1 * G::S;  // bytes between elements j, j+1 of one CTA
+        // CTA-local: task (x, n1) of a residue n1 this CTA holds, element j
+        // at local row (n1 - rank*N1C)*R2 + j
+        constexpr int TASKS = G::N1C * G::N;
+        const int n1b = G::rank() * G::N1C;
 #pragma unroll 1
         for (int tau = threadIdx.x; tau < TASKS; tau += G::NT) {
-            const int x = tau % G::N, n1 = n1b + tau / G::N;
-            const uint32_t off = sizeof(float2) * (uint32_t)(n1 * G::S + G::px(x));
+            const int x = tau % G::N, n1l = tau / G::N, n1 = n1b + n1l;
+            float2 *p = buf + n1l * R2 * G::S + G::px(x);
             float2 v[R2];
 #pragma unroll
-            for (int j = 0; j < R2; ++j) v[j] = ld_cluster(pb[j / JPC] + off + kRow * (j % JPC));
+            for (int j = 0; j < R2; ++j) v[j] = p[G::S * j];
             if constexpr (FWD) {
                 DFT<R2, SG>::run(v);
 #pragma unroll
@@ -471,7 +474,7 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
                 DFT<R2, SG>::run(v);
             }
 #pragma unroll
-            for (int j = 0; j < R2; ++j) st_cluster(pb[j / JPC] + off + kRow * (j % JPC), v[j]);
+            for (int j = 0; j < R2; ++j) p[G::S * j] = v[j];
         }
         return;
     }
@@ -507,23 +510,29 @@ __device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
     if constexpr (G::CL > 1) {
-        // CTA-local: the R1 rows of task (x, k2) are local rows R1*(k2 - k2b) + j
+        // distributed: CTA r owns the tasks k2 in [r*K2C, (r+1)*K2C) of every
+        // column; element j (row j + R1*k2, residue j) lives in CTA j / N1C at
+        // local row (j % N1C)*R2 + k2
         constexpr int K2C = R2 / G::CL;
         constexpr int TASKS = K2C * G::N;
+        uint32_t pb[G::CL];  // shared::cluster addresses of the CTAs' fields
+#pragma unroll
+        for (int r = 0; r < G::CL; ++r) pb[r] = peer_addr(buf, r);
         const int k2b = G::rank() * K2C;
+        constexpr uint32_t kRes = sizeof(float2) * R2 * G::S;  // bytes between residues of one CTA
 #pragma unroll 1
         for (int tau = threadIdx.x; tau < TASKS; tau += G::NT) {
-            const int x = tau % G::N, k2l = tau / G::N;
-            const int y0 = R1 * (k2b + k2l);
-            float2 *p = buf + R1 * k2l * G::S + G::px(x);
+            const int x = tau % G::N, k2 = k2b + tau / G::N;
+            const int y0 = R1 * k2;
+            const uint32_t off = sizeof(float2) * (uint32_t)(k2 * G::S + G::px(x));
             float2 v[R1];
 #pragma unroll
-            for (int j = 0; j < R1; ++j) v[j] = p[G::S * j];
+            for (int j = 0; j < R1; ++j) v[j] = ld_cluster(pb[j / G::N1C] + off + kRes * (j % G::N1C));
             if constexpr (IN != 0) DFT<R1, IN>::run(v);
             op(y0, x, v);
             if constexpr (OUT != 0) DFT<R1, OUT>::run(v);
 #pragma unroll
-            for (int j = 0; j < R1; ++j) p[G::S * j] = v[j];
+            for (int j = 0; j < R1; ++j) st_cluster(pb[j / G::N1C] + off + kRes * (j % G::N1C), v[j]);
         }
         return;
     }

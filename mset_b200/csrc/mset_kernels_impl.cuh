@@ -171,7 +171,7 @@ struct PositionKernel {
         sync_rows();
         for (int s = s0; s < s1; ++s) {
             row_passB<G, -1>(buf);
-            sync_all<G>();
+            sync_rowcol();
             col_passA<G, -1, true>(buf, tw);
             sync_cols<G>();
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -180,7 +180,7 @@ struct PositionKernel {
             });
             sync_cols<G>();
             col_passA<G, +1, false>(buf, tw);
-            sync_all<G>();
+            sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
             float2 *o = out + (size_t)(s - s0) * NN;
@@ -253,7 +253,7 @@ struct PositionKernel {
         });
         sync_cols<G>();
         col_passA<G, -1, false>(buf, tw);
-        sync_all<G>();
+        sync_rowcol();
         row_passB<G, -1>(buf);
         sync_rows();
         row_passA_pf<G, -1, -1, TPre<G>>(buf, tw, pf_t(0), [&](int y, int n1, float2 *v, const TPre<G> &pre) {
@@ -271,7 +271,7 @@ struct PositionKernel {
         if constexpr (METHOD == kMSET) {
             for (int s = 0; s < ns; ++s) {
                 row_passB<G, -1>(buf);
-                sync_all<G>();
+                sync_rowcol();
                 col_passA<G, -1, true>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -280,7 +280,7 @@ struct PositionKernel {
                 });
                 sync_cols<G>();
                 col_passA<G, +1, false>(buf, tw);
-                sync_all<G>();
+                sync_rowcol();
                 row_passB<G, +1>(buf);
                 sync_rows();
                 const bool last = s + 1 == ns;
@@ -313,7 +313,7 @@ struct PositionKernel {
 
         // ---- far field, error, residual (mset.cu:186-227) ----
         row_passB<G, -1>(buf);
-        sync_all<G>();
+        sync_rowcol();
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
         double err = 0.0;
@@ -392,7 +392,7 @@ struct PositionKernel {
             // the saved wave was written long ago (DRAM); have it in L2 by the row pass
             prefetch_l2(wave, (unsigned)(sizeof(float2) * NN));
             col_passA<G, +1, false>(buf, tw);
-            sync_all<G>();
+            sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
             auto pf = [&](int y, int n1, TSPre<G> &pre) {
@@ -433,7 +433,7 @@ struct PositionKernel {
                 row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop);
                 sync_rows();
                 row_passB<G, -1>(buf);
-                sync_all<G>();
+                sync_rowcol();
                 col_passA<G, -1, true>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -453,9 +453,9 @@ struct PositionKernel {
         //      (mset.cu:316-327; utility.cu:829-876) ----
         double pdx = 0.0, pdy = 0.0;
         if constexpr (ADJ == kREF) {
-            const int yb = G::row0();
+            const int yb = G::ybase();
             for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
-                const int yl = i / N, x = i % N, y = yb + yl;
+                const int yl = i / N, x = i % N, y = G::gy(yb, yl);
                 const float2 c0 = buf[G::at(yl, x)];
                 const float2 *f = save + (size_t)y * N + x;
                 float2 dx, dy;
@@ -477,7 +477,7 @@ struct PositionKernel {
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         sync_rows();
         row_passB<G, +1>(buf);
-        sync_all<G>();
+        sync_rowcol();
         col_passA<G, +1, true>(buf, tw);
         sync_cols<G>();
         const float inv = 1.0f / (float)NN;
@@ -667,14 +667,15 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
     for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
     sync_all<G>();  // (cluster) every CTA has started before any remote access
     constexpr int N = G::N;
-    const int yb = G::row0();
+    const int yb = G::ybase();
     if constexpr (TO_Q) {
-        for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) buf[G::at(i / N, i % N)] = in[(size_t)yb * N + i];
+        for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT)
+            buf[G::at(i / N, i % N)] = in[(size_t)G::gy(yb, i / N) * N + i % N];
         __syncthreads();
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         __syncthreads();
         row_passB<G, +1>(buf);
-        sync_all<G>();
+        sync_rowcol();
         col_passA<G, +1, true>(buf, tw);
         sync_all<G>();
         const float inv = 1.0f / (float)(N * N);
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
         });
         sync_all<G>();
         col_passA<G, -1, false>(buf, tw);
-        sync_all<G>();
+        sync_rowcol();
         row_passB<G, -1>(buf);
         __syncthreads();
         row_passA<G, -1, 0>(buf, tw, [&](int y, int n1, float2 *v) {
@@ -812,6 +813,8 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
 // a field split by rows over a cluster of CL_ CTAs
 #define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
+#define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_) \
+    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
 #define MSET_UNPAREN(...) __VA_ARGS__
 #define MSET_DEFINE_GEO_T(NAME_, N_, R1_, GT_)                                         \
     namespace mset {                                                                   \

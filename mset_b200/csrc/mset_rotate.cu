@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
     }
     const float inv = 1.0f / (float)(N * N);
     // one plane per CTA, or per cluster when the plane is split by rows
-    const int y_lo = G::row0();
+    const int yb = G::ybase();
     sync_all<G>();  // (cluster) every CTA has started before any remote access
     for (int c = blockIdx.x / G::CL; c < N; c += gridDim.x / G::CL) {
         bool qc;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
             // fourth shear's real() acts
             if (REAL) {
                 for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
-                    float2 *p = S + (long)c * sc + (long)(y_lo + i / N) * sy + (long)(i % N) * sx;
+                    float2 *p = S + (long)c * sc + (long)G::gy(yb, i / N) * sy + (long)(i % N) * sx;
                     p->y = 0.f;
                 }
             }
@@ -122,13 +122,13 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
         }
         for (int i = threadIdx.x; i < G::ROWS * N; i += G::NT) {
             const int yy = i / N, xx = i % N;
-            buf[G::at(yy, xx)] = S[(long)c * sc + (long)(y_lo + yy) * sy + (long)xx * sx];
+            buf[G::at(yy, xx)] = S[(long)c * sc + (long)G::gy(yb, yy) * sy + (long)xx * sx];
         }
         __syncthreads();
         row_passA<G, 0, -1>(buf, tw, NoOp{});
         sync_rows();
         row_passB<G, -1>(buf);
-        sync_all<G>();
+        sync_rowcol();
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
         col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
         });
         sync_cols<G>();
         col_passA<G, +1, false>(buf, tw);
-        sync_all<G>();
+        sync_rowcol();
         row_passB<G, +1>(buf);
         sync_rows();
         row_passA<G, +1, 0>(buf, tw, NoOp{});
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(G::NT, 1) k_shear(float2 *S, const float2 *twn
             const int yy = i / N, xx = i % N;
             float2 v = buf[G::at(yy, xx)];
             if (REAL) v.y = 0.f;
-            S[(long)c * sc + (long)(y_lo + yy) * sy + (long)xx * sx] = v;
+            S[(long)c * sc + (long)G::gy(yb, yy) * sy + (long)xx * sx] = v;
         }
         sync_all<G>();
         (void)R2;

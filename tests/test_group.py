@@ -159,7 +159,7 @@ def test_group_rejects_a_repeated_member(gpu_available):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [64, 96, 128, 160])
+@pytest.mark.parametrize("n", [64, 96, 128, 160, 256])
 def test_every_kernel_shape_matches_default_and_oracle(gpu_available, n):
     """the alternative thread shapes of a window (the autotuner's choices)
     give the default shape's results and the oracle's"""
