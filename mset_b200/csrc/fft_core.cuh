@@ -24,6 +24,7 @@
 // so one propagation slab costs six shared-memory round trips, with a
 // CTA-wide barrier only where row passes meet column passes.
 #pragma once
+#include <type_traits>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -277,9 +278,9 @@ struct Geo {
 // cluster through distributed shared memory, each task owned by one thread so
 // that the pass is in place.  One distributed pass per column transform, and
 // the switch between row passes and column pass A needs only a CTA barrier.
-template <int N_, int R1_, int NT_, int CL_>
-struct GeoCl : Geo<N_, R1_, NT_, 1> {
-    using Base = Geo<N_, R1_, NT_, 1>;
+template <int N_, int R1_, int NT_, int CL_, int MINB_ = 1>
+struct GeoCl : Geo<N_, R1_, NT_, MINB_> {
+    using Base = Geo<N_, R1_, NT_, MINB_>;
     static constexpr int CL = CL_;
     static constexpr int ROWS = N_ / CL_;
     static constexpr int N1C = R1_ / CL_;  // residues n1 per CTA
@@ -391,6 +392,16 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
     constexpr bool ahead = Pre::kAhead;
     Pre pre, nxt;
     if (ahead && O::lane() < TASKS) pf(G::gy(yb, yl0 + O::lane() / R1), O::lane() % R1, pre);
+    // a lane's residue n1 is the same in every task when R1 divides 32, so
+    // its twiddles W^(n1 k2) stay in registers for the whole pass instead of
+    // being read from shared memory twice per task (while R2 <= 8 leaves
+    // room for them)
+    constexpr bool kTwReg = (32 % R1 == 0) && R2 <= 8 && (IN != 0 || OUT != 0);
+    float2 twr[kTwReg ? R2 : 1];
+    if constexpr (kTwReg) {
+#pragma unroll
+        for (int k2 = 1; k2 < R2; ++k2) twr[k2] = tw[k2 * R1 + O::lane() % R1];
+    }
 #pragma unroll 1
     for (int tau = O::lane(); tau < TASKS; tau += 32) {
         const int n1 = tau % R1, y = G::gy(yb, yl0 + tau / R1);
@@ -403,16 +414,21 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
         float2 v[R2];
 #pragma unroll
         for (int j = 0; j < R2; ++j) v[j] = row[(R1 + 1) * j];
+        auto twi = [&](int k2, auto sg) -> float2 {
+            constexpr int SG = decltype(sg)::value;
+            if constexpr (kTwReg) return SG < 0 ? twr[k2] : cconj(twr[k2]);
+            else return twN<G, SG>(tw, n1, k2);
+        };
         if constexpr (IN != 0) {
 #pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, IN>(tw, n1, k2));
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, IN>{}));
             DFT<R2, IN>::run(v);
         }
         op(y, n1, v, pre);
         if constexpr (OUT != 0) {
             DFT<R2, OUT>::run(v);
 #pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, OUT>(tw, n1, k2));
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, OUT>{}));
         }
 #pragma unroll
         for (int j = 0; j < R2; ++j) row[(R1 + 1) * j] = v[j];

@@ -1425,7 +1425,7 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
     for (int v = 0; v < plan_variants(s->n); ++v) {
         Plan pl;
         if (!plan_for(s->n, &pl, v)) continue;
-        pl.max_clusters = plan_in.max_clusters;
+        if (pl.cl > 1) pl.max_clusters = pl.ops->max_clusters();
         s->plan = pl;
         const int occ = occupancy_limit(s);
         int last_grid = 0;
@@ -1639,7 +1639,7 @@ int mset_batch_set_variant(mset_session *s, int variant) {
     Plan pl;
     if (variant < 0 || !plan_for(s->n, &pl, variant))
         return fail(MSET_E_ARG, "window %d has %d kernel shapes, not %d", s->n, plan_variants(s->n), variant + 1);
-    pl.max_clusters = s->plan.max_clusters;
+    if (pl.cl > 1) pl.max_clusters = pl.ops->max_clusters();
     s->plan = pl;
     s->tuned_grid = 0;
     s->tuned_us_per_pos = 0;

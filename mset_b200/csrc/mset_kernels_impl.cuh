@@ -395,6 +395,9 @@ struct PositionKernel {
             sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
+            // both operands are loaded before the task's shared-memory reads:
+            // loading either inside the op instead (fewer live registers at
+            // R2 = 16) exposes its latency and cost 17-22% at n = 256
             auto pf = [&](int y, int n1, TSPre<G> &pre) {
                 const float2 *sv = wave + (size_t)y * N + n1;
 #pragma unroll
@@ -813,8 +816,8 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
 // a field split by rows over a cluster of CL_ CTAs
 #define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
-#define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_) \
-    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
+#define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_, MINB_) \
+    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_, MINB_>))
 #define MSET_UNPAREN(...) __VA_ARGS__
 #define MSET_DEFINE_GEO_T(NAME_, N_, R1_, GT_)                                         \
     namespace mset {                                                                   \
