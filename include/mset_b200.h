@@ -105,6 +105,43 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
  * positions, error accumulated and normalised as mex_main.cu:179. */
 int mset_error(mset_session *s, int mode, float *error_out);
 
+/* ---- per-position steps of the reference's CPU path -----------------------
+ * STEP02_FORWARD_4D(_SSET) and STEP03_BACK(_SSET) for one position of the
+ * uploaded tilt (src/STEP02_FORWARD_4D.m:6-51, src/STEP03_BACK.m:6-39, called
+ * from Run_MSET_recon.m:136-157), computed by the same fused kernel as
+ * mset_run.  Real-space arrays are MATLAB's centred ones; spectra come back
+ * centred (fftshift) as in the MATLAB code.  The probe shift follows the CUDA
+ * module (IFFT -> phase -> FFT), which differs from the MATLAB path only on
+ * the Nyquist lines of even windows at sub-pixel positions.
+ *
+ * mset_forward_position (STEP02): position k (0-based; selects the measured
+ * pattern) at scan coordinates (row, col) (1-based pixels, STEM_data.row /
+ * .col).  Every output may be NULL:
+ *   calc_out  float [n][n]          |Psi|^2, centred (calculated_4D_data{k})
+ *   resi_out  float [n][n][2]       residual, centred (resi_vec)
+ *   waves_out float [ns][n][n][2]   wave after each slab (save_wave_f);
+ *                                   SSET: [1][n][n][2], the shifted probe
+ *   psi0_out  float [n][n][2]       shifted probe (tmp_probe_wave)
+ *   err_out   float                 this position's error term,
+ *                                   mean((sqrt(I_meas) - |Psi|)^2) / (N_scan_x N_scan_y)
+ * The waves, the residual and (row, col) stay in the session for the
+ * adjoint. */
+int mset_forward_position(mset_session *s, int mode, int k, float row, float col, float *calc_out,
+                          float *resi_out, float *waves_out, float *psi0_out, float *err_out);
+/* mset_adjoint_position (STEP03, and STEP04 when update_rvol != 0): back-
+ * propagates the residual of the preceding mset_forward_position of the same
+ * mode, or resi_in (float [n][n][2], centred) when not NULL.  Updates the
+ * session's probe as STEP03 does (probe -= step_size[1] shift(chi0)); with
+ * update_rvol also RVol += step_size[0] Re(grad) (Run_MSET_recon.m:155).
+ * Outputs (may be NULL):
+ *   grad_out   float [nz][n][n][2]  i conj(T) conj(psi) chi per voxel, the slab's
+ *                                   value on each of its voxels (STEM_data.grad)
+ *   probe_out  float [n][n][2]      the updated probe
+ *   rowcol_out float [2]            the updated scan coordinates (row, col)
+ * A forward is consumed by one adjoint. */
+int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *resi_in, int update_rvol,
+                          float *grad_out, float *probe_out, float *rowcol_out);
+
 /* global-session shims with the MEX's lifetime (one implicit session per
  * process, recreated by every upload, mex_main.cu:13, 56) */
 int mset_mex_upload(const mset_upload_args *a);

@@ -36,6 +36,8 @@ SIGNATURES = {
     "mset_run": (C.c_int, [C.c_void_p, C.c_int, _F, _F, _F, _F, _F]),
     "mset_run_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F, _F, _F, _F, _F]),
     "mset_error": (C.c_int, [C.c_void_p, C.c_int, _F]),
+    "mset_forward_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, _F, _F, _F, _F, _F]),
+    "mset_adjoint_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F, C.c_int, _F, _F, _F]),
     "mset_mex_upload": (C.c_int, [C.c_void_p]),
     "mset_mex_run": (C.c_int, [C.c_int, _F, _F, _F, _F, _F]),
     "mset_mex_error": (C.c_int, [C.c_int, _F]),

@@ -151,6 +151,12 @@ struct mset_session {
     DevBuf<float> tv_in, tv_out, tv_P, tv_Y, tv_D;
     DevBuf<double> tv_err;
     // rotation work buffers
+    // per-position steps (mset_forward_position / mset_adjoint_position)
+    DevBuf<float2> step_resi, step_grad;
+    DevBuf<float> step_calc, step_pos;
+    DevBuf<double> step_err;
+    int step_k = -1, step_mode = 0;  // position and method of the pending STEP02 (-1: none)
+    float step_x = 0, step_y = 0;
     DevBuf<float> rot_vol;
     DevBuf<float2> rot_S, rot_tw;
     int rot_n = 0;
@@ -460,6 +466,7 @@ int mset_upload(mset_session *s, const mset_upload_args *a) {
     if (rc) return rc;
     s->ready = false;
     s->batch = false;
+    s->step_k = -1;
     rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
     if (rc) return rc;
     s->step[0] = a->step_size[0];
@@ -554,6 +561,140 @@ int mset_error(mset_session *s, int mode, float *error_out) {
     CK(cudaStreamSynchronize(s->st));
     const double n2 = (double)s->n * s->n;
     *error_out = (float)(e / ((double)s->nsx * s->nsy) / n2);  // mex_main.cu:179
+    return 0;
+}
+
+// ---- per-position steps (STEP02_FORWARD_4D / STEP03_BACK) ---------------------
+
+// centred (MATLAB fftshift) index of scrambled location L: frequency scr(L)
+// moved by floor(n/2)
+static int centred_of_scrambled(int L, int n, int r1) {
+    const int k = L / r1 + (n / r1) * (L % r1);
+    int c = k - (n + 1) / 2;
+    return c < 0 ? c + n : c;
+}
+
+int mset_forward_position(mset_session *s, int mode, int k, float row, float col, float *calc_out,
+                          float *resi_out, float *waves_out, float *psi0_out, float *err_out) {
+    Range range_("mset_forward_position");
+    if (!s) return fail(MSET_E_ARG, "null session");
+    int rc = check_mode(mode);
+    if (rc) return rc;
+    if (!s->ready || s->batch) return fail(MSET_E_STATE, "forward_position called before upload");
+    TiltBufs &t = s->tilts[0];
+    if (k < 0 || k >= t.npos) return fail(MSET_E_ARG, "position %d out of range (%d positions)", k, t.npos);
+    if (!std::isfinite(row) || !std::isfinite(col)) return fail(MSET_E_ARG, "non-finite scan coordinates");
+    rc = set_device(s);
+    if (rc) return rc;
+    s->step_k = -1;
+    rc = ensure_save(s, 1);
+    if (!rc) rc = refresh_tilt_table(s);
+    if (rc) return rc;
+    const int n = s->n;
+    const size_t n2 = (size_t)n * n;
+    const int ns = mode == MSET_MODE_SSET ? 1 : s->ns;
+    CK(s->step_resi.ensure(n2));
+    CK(s->step_calc.ensure(n2));
+    CK(s->step_err.ensure(1));
+    CK(cudaMemsetAsync(s->step_err.p, 0, sizeof(double), s->st));
+    LaunchArgs a = base_args(s);
+    a.step_phase = 1;
+    a.step_k = k;
+    a.step_x = row;
+    a.step_y = col;
+    a.step_resi = s->step_resi.p;
+    a.step_calc = s->step_calc.p;
+    a.step_err = s->step_err.p;
+    CKL(launch_positions(s->plan, mode, kREF, kStep, a, std::max(1, s->plan.cl), s->st), "STEP02 launch");
+    // the waves of field 0: slot 0 = psi0, slot s + 1 = wave after slab s
+    std::vector<float2> resi(resi_out ? n2 : 0);
+    if (resi_out)
+        CK(cudaMemcpyAsync(resi.data(), s->step_resi.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    if (calc_out) CK(cudaMemcpyAsync(calc_out, s->step_calc.p, sizeof(float) * n2, cudaMemcpyDeviceToHost, s->st));
+    if (waves_out) {
+        // STEP02_FORWARD_4D.m:33 (after each slab); SSET: psi0 (STEP02_FORWARD_4D_SSET.m:16)
+        const float2 *src = s->save.p + (mode == MSET_MODE_SSET ? 0 : n2);
+        CK(cudaMemcpyAsync(waves_out, src, sizeof(float2) * n2 * ns, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (psi0_out) CK(cudaMemcpyAsync(psi0_out, s->save.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    double e = 0;
+    CK(cudaMemcpyAsync(&e, s->step_err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (resi_out) {
+        float2 *ro = reinterpret_cast<float2 *>(resi_out);
+        for (int Ly = 0; Ly < n; ++Ly) {
+            const int r = centred_of_scrambled(Ly, n, s->plan.r1);
+            for (int Lx = 0; Lx < n; ++Lx)
+                ro[(size_t)r * n + centred_of_scrambled(Lx, n, s->plan.r1)] = resi[(size_t)Ly * n + Lx];
+        }
+    }
+    // mean over the pattern / (N_scan_x N_scan_y)  (STEP02_FORWARD_4D.m:46-48)
+    if (err_out) *err_out = (float)(e / (double)n2 / ((double)s->nsx * s->nsy));
+    s->step_k = k;
+    s->step_mode = mode;
+    s->step_x = row;
+    s->step_y = col;
+    return 0;
+}
+
+int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *resi_in, int update_rvol,
+                          float *grad_out, float *probe_out, float *rowcol_out) {
+    Range range_("mset_adjoint_position");
+    if (!s) return fail(MSET_E_ARG, "null session");
+    int rc = check_mode(mode);
+    if (rc) return rc;
+    if (adjoint != MSET_ADJOINT_REF && adjoint != MSET_ADJOINT_EXACT) return fail(MSET_E_ARG, "bad adjoint mode");
+    if (!s->ready || s->batch) return fail(MSET_E_STATE, "adjoint_position called before upload");
+    if (s->step_k < 0 || s->step_mode != mode)
+        return fail(MSET_E_STATE, "adjoint_position needs a preceding forward_position of the same mode");
+    rc = set_device(s);
+    if (rc) return rc;
+    const int n = s->n;
+    const size_t n2 = (size_t)n * n;
+    const int ns = mode == MSET_MODE_SSET ? 1 : s->ns;
+    if (resi_in) {
+        const float2 *ri = reinterpret_cast<const float2 *>(resi_in);
+        std::vector<float2> scr(n2);
+        for (int Ly = 0; Ly < n; ++Ly) {
+            const int r = centred_of_scrambled(Ly, n, s->plan.r1);
+            for (int Lx = 0; Lx < n; ++Lx)
+                scr[(size_t)Ly * n + Lx] = ri[(size_t)r * n + centred_of_scrambled(Lx, n, s->plan.r1)];
+        }
+        CK(cudaMemcpyAsync(s->step_resi.p, scr.data(), sizeof(float2) * n2, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    CK(s->step_grad.ensure(n2 * ns));
+    CK(s->step_pos.ensure(2));
+    LaunchArgs a = base_args(s);
+    a.step_phase = 2;
+    a.step_k = s->step_k;
+    a.step_x = s->step_x;
+    a.step_y = s->step_y;
+    a.step04 = update_rvol ? 1 : 0;
+    a.step_resi = s->step_resi.p;
+    a.step_grad = s->step_grad.p;
+    a.step_pos = s->step_pos.p;
+    CKL(launch_positions(s->plan, mode, adjoint, kStep, a, std::max(1, s->plan.cl), s->st), "STEP03 launch");
+    TiltBufs &t = s->tilts[0];
+    std::vector<float2> g(grad_out ? n2 * ns : 0);
+    if (grad_out)
+        CK(cudaMemcpyAsync(g.data(), s->step_grad.p, sizeof(float2) * n2 * ns, cudaMemcpyDeviceToHost, s->st));
+    if (probe_out) {
+        CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
+        CK(cudaMemcpyAsync(probe_out, s->tmpc.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (rowcol_out) CK(cudaMemcpyAsync(rowcol_out, s->step_pos.p, sizeof(float) * 2, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (grad_out) {
+        // the slab's value on each of its voxels (STEP03_BACK.m:18-22; SSET: every z,
+        // STEP03_BACK_SSET.m:13-14)
+        float2 *go = reinterpret_cast<float2 *>(grad_out);
+        for (int z = 0; z < s->nz; ++z) {
+            const int sl = mode == MSET_MODE_SSET ? 0 : z / s->b;
+            std::memcpy(go + (size_t)z * n2, g.data() + (size_t)sl * n2, sizeof(float2) * n2);
+        }
+    }
+    s->step_k = -1;
     return 0;
 }
 

@@ -15,7 +15,9 @@ enum Mode {
     kErr = 2,    // forward + error only (run_error_mset / run_error_sset)
     kSim = 3,    // forward + write |Psi|^2 (centred layout)
     kBatchCentred = 4,  // kBatch reading the caller's centred intensities (no prepared amplitudes)
-    kBatchCk = 5        // kBatch keeping every k-th wave and recomputing the rest (checkpointing)
+    kBatchCk = 5,       // kBatch keeping every k-th wave and recomputing the rest (checkpointing)
+    kStep = 6           // one position as the reference's per-position steps: STEP02 (forward;
+                        // residual, |Psi|^2 and waves out) or STEP03 (adjoint from a residual)
 };
 
 // one tilt: all buffers on the device
@@ -51,6 +53,16 @@ struct LaunchArgs {
     int seq_tilt;           // kSeq: index of the tilt to run
     int ckpt;               // 0: keep every slab's wave; k: keep every k-th, recompute the rest
     int slots;              // saved-wave slots (n x n complex) per field
+    // kStep: one position (index step_k of tilt seq_tilt) at scan coordinates
+    // (step_x, step_y); phase 1 = STEP02, phase 2 = STEP03
+    int step_phase, step_k;
+    int step04;             // STEP03 also applies RVol += step0 * Re(grad) (STEP04)
+    float step_x, step_y;
+    float2 *step_resi;      // [n][n] residual, scrambled (STEP02 writes it, STEP03 reads it)
+    float *step_calc;       // [n][n] |Psi|^2, centred (STEP02)
+    float2 *step_grad;      // [ns][n][n] complex gradient i conj(T) conj(psi) chi (STEP03)
+    float *step_pos;        // [2] updated scan coordinates (STEP03)
+    double *step_err;       // [1] += sum over pixels of (A - M)^2 (STEP02; zeroed by the host)
 };
 
 // saved-wave slots a CTA needs for ns slabs with checkpoint interval k

@@ -223,7 +223,14 @@ struct PositionKernel {
         float2 *recbuf = save + (size_t)nseg * NN;
         float2 *park = save + (size_t)(nseg + ck) * NN;
         float *V = t.V;
-        const float sxp = t.sx[p], syp = t.sy[p];
+        float sxp, syp;
+        if constexpr (MODE == kStep) {
+            sxp = a.step_x;
+            syp = a.step_y;
+        } else {
+            sxp = t.sx[p];
+            syp = t.sy[p];
+        }
         const float s1 = syp - a.center, s2 = sxp - a.center;  // mset.cu:121
         // separable Fourier shift factor, indexed by scrambled location
         for (int L = threadIdx.x; L < N; L += G::NT) {
@@ -244,6 +251,10 @@ struct PositionKernel {
             };
         };
 
+        double err = 0.0;
+        // kStep phase 2 (STEP03) starts from a residual and skips the forward
+        const bool fwd = MODE != kStep || a.step_phase == 1;
+        if (fwd) {
         // ---- incident wave psi0 = F(Q . fs)  (mset.cu:110-131) ----
         col_passB<G, 0, -1>(buf, [&](int y0, int x, float2 *v) {
             const float2 *q = t.Q + (size_t)y0 * N + x;
@@ -294,8 +305,11 @@ struct PositionKernel {
                         if constexpr (MODE != kSim && MODE != kErr) {
                             const int w = s + 1;
                             float2 *sv = nullptr;
-                            if (!ck) sv = save + (size_t)w * NN;
-                            else if (w % ck == 0 && w < ns) sv = save + (size_t)(w / ck) * NN;
+                            if (!ck) {
+                                sv = save + (size_t)w * NN;
+                            } else if constexpr (MODE == kBatchCk) {
+                                if (w % ck == 0 && w < ns) sv = save + (size_t)(w / ck) * NN;
+                            }
                             if (sv) {
                                 sv += (size_t)y * N + n1;
 #pragma unroll
@@ -316,7 +330,6 @@ struct PositionKernel {
         sync_rowcol();
         col_passA<G, -1, true>(buf, tw);
         sync_cols<G>();
-        double err = 0.0;
         const float *amp = t.amp ? t.amp + (size_t)p * NN : nullptr;
         const unsigned short *ampb = t.ampb ? t.ampb + (size_t)p * NN : nullptr;
         if constexpr (MODE == kSim || MODE == kErr) {
@@ -346,6 +359,30 @@ struct PositionKernel {
             }
             sync_all<G>();
             return;
+        } else if constexpr (MODE == kStep) {
+            // STEP02 (STEP02_FORWARD_4D.m:36-49): residual (scrambled) and
+            // |Psi|^2 (centred) out, error sum; the waves stay in the slots
+            col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+                for (int j = 0; j < R1; ++j) {
+                    const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
+                    const float A = sqrtf(a2 + 1e-30f);
+                    const float M = meas_amp(amp, ampb, y0 + j, x);
+                    const float d = A - M;
+                    err += (double)(d * d);
+                    a.step_resi[(size_t)(y0 + j) * N + x] = cscale(v[j], 1.0f - M / A);
+                    const int h = (N + 1) / 2;
+                    int r = G::scr(y0 + j) - h, c = G::scr(x) - h;
+                    if (r < 0) r += N;
+                    if (c < 0) c += N;
+                    a.step_calc[(size_t)r * N + c] = a2;
+                }
+            });
+            double dummy = 0.0;
+            block_sum2<G::NT>(err, dummy, red);
+            if (threadIdx.x == 0) atomicAdd(a.step_err, err);
+            sync_all<G>();
+            return;
         } else {
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
@@ -362,6 +399,19 @@ struct PositionKernel {
                         r = cscale(r, 1.0f / (float)NN);
                     }
                     v[j] = r;
+                }
+            });
+            sync_cols<G>();
+        }
+        } else {
+            // STEP03 (STEP03_BACK.m:10-13): the residual r conj(P) / N^2
+            // (SSET: r / N^2), inverse column transform started
+            col_passB<G, 0, +1>(buf, [&](int y0, int x, float2 *v) {
+#pragma unroll
+                for (int j = 0; j < R1; ++j) {
+                    const float2 r = a.step_resi[(size_t)(y0 + j) * N + x];
+                    if constexpr (METHOD == kMSET) v[j] = cmulc(r, prop(a, py, px, y0 + j, x));
+                    else v[j] = cscale(r, 1.0f / (float)NN);
                 }
             });
             sync_cols<G>();
@@ -426,6 +476,22 @@ struct PositionKernel {
                         // RVol += step0 * Re(grad), slab-replicated (mset.cu:273-284)
                         const float du = a.step0 * gre;
                         for (int z = z0; z < z1; ++z) V[(size_t)z * NN + (size_t)y * N + x] += du;
+                    } else if constexpr (MODE == kStep) {
+                        // STEP03_BACK.m:15-16: g = i u, kept complex
+                        a.step_grad[(size_t)s * NN + (size_t)y * N + x] = make_float2(gre, u.x);
+                        if (a.step04) {
+                            int z0, z1;
+                            if constexpr (METHOD == kSSET) {
+                                z0 = 0;
+                                z1 = a.nz;
+                            } else {
+                                z0 = s * a.b;
+                                z1 = min(z0 + a.b, a.nz);
+                            }
+                            // Run_MSET_recon.m:155
+                            const float du = a.step0 * gre;
+                            for (int z = z0; z < z1; ++z) V[(size_t)z * NN + (size_t)y * N + x] += du;
+                        }
                     } else {
                         atomicAdd(t.grad + (size_t)s * NN + (size_t)y * N + x, (double)gre);
                     }
@@ -502,7 +568,7 @@ struct PositionKernel {
                     pdx -= (double)(Xx.x * v[j].x + Xx.y * v[j].y);
                     pdy -= (double)(Xy.x * v[j].x + Xy.y * v[j].y);
                 }
-                if constexpr (MODE == kSeq) {
+                if constexpr (MODE == kSeq || MODE == kStep) {
                     float2 q = t.Q[li];
                     q.x -= a.step1 * d.x;
                     q.y -= a.step1 * d.y;
@@ -538,6 +604,9 @@ struct PositionKernel {
             if constexpr (MODE == kSeq) {
                 t.sx[p] = sxp + a.step2 * (float)pdx;  // mset.cu:322
                 t.sy[p] = syp + a.step2 * (float)pdy;  // mset.cu:327
+            } else if constexpr (MODE == kStep) {
+                a.step_pos[0] = sxp + a.step2 * (float)pdx;  // STEP03_BACK.m:37-38
+                a.step_pos[1] = syp + a.step2 * (float)pdy;
             } else {
                 t.posdir[2 * p] = pdx;
                 t.posdir[2 * p + 1] = pdy;
@@ -581,6 +650,10 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
         if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
         sync_all<G>();
         for (int p = 0; p < s_tilt.npos; ++p) K::run(a, s_tilt, p, buf, save, red);
+    } else if constexpr (MODE == kStep) {
+        if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
+        sync_all<G>();
+        K::run(a, s_tilt, a.step_k, buf, save, red);
     } else {
         int cur = -1;
         for (;;) {
@@ -777,6 +850,7 @@ int geo_positions(int method, int adjoint, int mode, const LaunchArgs &a, int gr
     MSET_L(kSSET, kREF, kSeq) MSET_L(kSSET, kREF, kBatch) MSET_L(kSSET, kEXACT, kSeq) MSET_L(kSSET, kEXACT, kBatch)
     MSET_L(kMSET, kREF, kErr) MSET_L(kSSET, kREF, kErr) MSET_L(kMSET, kREF, kSim) MSET_L(kSSET, kREF, kSim)
     MSET_L(kMSET, kREF, kBatchCk) MSET_L(kMSET, kEXACT, kBatchCk)
+    MSET_L(kMSET, kREF, kStep) MSET_L(kMSET, kEXACT, kStep) MSET_L(kSSET, kREF, kStep) MSET_L(kSSET, kEXACT, kStep)
 #undef MSET_L
     return (int)cudaErrorInvalidValue;
 }

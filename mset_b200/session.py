@@ -47,6 +47,7 @@ class Session:
         self._h = h
         self._keep: list = []
         self.n = self.nz = self.npos = 0
+        self._binning = 1
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -127,6 +128,7 @@ class Session:
         self._keep = [rvol, pr, pp, sx, sy, meas]
         check("mset_upload", self._lib.mset_upload(self._h, C.byref(a)))
         self.n, self.nz, self.npos = n1, nz, npos
+        self._binning = int(slice_binning)
 
     # ---- 'run_mset' / 'run_sset' (mex_main.cu:98-155) ----
     def run(self, mode: int = MSET_MODE_MSET, adjoint: int = MSET_ADJOINT_REF, with_error: bool = True):
@@ -146,6 +148,47 @@ class Session:
         err = np.zeros(1, np.float32)
         check("mset_error", self._lib.mset_error(self._h, int(mode), fptr(err)))
         return float(err[0])
+
+    # ---- per-position steps of the CPU path (Run_MSET_recon.m:136-157) ----
+    def step02(self, k: int, row: float, col: float, mode: int = MSET_MODE_MSET) -> dict:
+        """STEP02_FORWARD_4D(_SSET) of position k at scan coordinates (row, col):
+        dict with calc (centred |Psi|^2), resi (centred residual), waves
+        (save_wave_f: [ns][n][n], SSET [1][n][n]), psi0 (tmp_probe_wave) and
+        err (this position's error term)"""
+        n = self.n
+        ns = 1 if mode == MSET_MODE_SSET else self._ns()
+        calc = np.empty((n, n), np.float32)
+        resi = np.empty((n, n, 2), np.float32)
+        waves = np.empty((ns, n, n, 2), np.float32)
+        psi0 = np.empty((n, n, 2), np.float32)
+        err = np.zeros(1, np.float32)
+        check("mset_forward_position",
+              self._lib.mset_forward_position(self._h, int(mode), int(k), float(row), float(col), fptr(calc),
+                                              fptr(resi), fptr(waves), fptr(psi0), fptr(err)))
+        cplx = lambda a: a.view(np.complex64)[..., 0]
+        return dict(calc=calc, resi=cplx(resi), waves=cplx(waves), psi0=cplx(psi0), err=float(err[0]))
+
+    def step03(self, mode: int = MSET_MODE_MSET, adjoint: int = MSET_ADJOINT_REF, resi=None,
+               update_rvol: bool = False) -> dict:
+        """STEP03_BACK(_SSET) after :meth:`step02` (and STEP04 with update_rvol):
+        dict with grad ([nz][n][n] complex, slab-replicated), probe (updated)
+        and row, col (updated scan coordinates)"""
+        n = self.n
+        ri = None if resi is None else _cplx_f32(resi)
+        if ri is not None and ri.shape != (n, n, 2):
+            raise ValueError("resi must be n x n complex")
+        grad = np.empty((self.nz, n, n, 2), np.float32)
+        probe = np.empty((n, n, 2), np.float32)
+        rc = np.zeros(2, np.float32)
+        check("mset_adjoint_position",
+              self._lib.mset_adjoint_position(self._h, int(mode), int(adjoint), fptr(ri) if ri is not None else None,
+                                              int(bool(update_rvol)), fptr(grad), fptr(probe), fptr(rc)))
+        cplx = lambda a: a.view(np.complex64)[..., 0]
+        return dict(grad=cplx(grad), probe=cplx(probe), row=float(rc[0]), col=float(rc[1]))
+
+    def _ns(self) -> int:
+        b = max(1, min(self._binning, self.nz))
+        return -(-self.nz // b)
 
 
 # ---------------------------------------------------------------------------

@@ -459,12 +459,14 @@ int orc_run_tilt(int n, int nz, int binning, double sigma, double dz, const doub
  * parity).  Any output pointer may be NULL.
  *   V [nz][n][n], probe/prop interleaved complex, amp_std = sqrt(ifftshift(I))
  *   psi0_out, far_out, chi0_out, probe_dir_out: interleaved complex N^2
- *   grad_out: ns slabs interleaved complex; pos_dir_out: 2 doubles; err_out: 1 */
+ *   grad_out: ns slabs interleaved complex; pos_dir_out: 2 doubles; err_out: 1
+ *   waves_out: ns+1 waves interleaved complex, [0] = psi0, [s+1] = wave after
+ *   slab s (save_wave_f of STEP02_FORWARD_4D.m:33; SSET: psi0 and T psi0) */
 int orc_position(int n, int nz, int binning, double sigma, double dz, int method, int admode,
                  const double *V, const double *probe, const double *prop_centered_d,
                  double scan_x, double scan_y, const double *amp_std,
                  double *psi0_out, double *far_out, double *err_out, double *grad_out,
-                 double *chi0_out, double *probe_dir_out, double *pos_dir_out) {
+                 double *chi0_out, double *probe_dir_out, double *pos_dir_out, double *waves_out) {
     long n2 = (long)n * n;
     float *propf = malloc(sizeof(float) * 2 * n2);
     model m;
@@ -488,6 +490,7 @@ int orc_position(int n, int nz, int binning, double sigma, double dz, int method
     if (chi0_out) memcpy(chi0_out, r.chi0, sizeof(cd) * n2);
     if (probe_dir_out) memcpy(probe_dir_out, r.probe_dir, sizeof(cd) * n2);
     if (pos_dir_out) { pos_dir_out[0] = r.pos_dir[0]; pos_dir_out[1] = r.pos_dir[1]; }
+    if (waves_out) memcpy(waves_out, r.waves, sizeof(cd) * n2 * (ns + 1));
     posres_free(&r);
     model_free(&m);
     return 0;

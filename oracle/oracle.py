@@ -33,7 +33,7 @@ def lib() -> C.CDLL:
         L.orc_run_tilt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _D, C.c_int, C.c_int,
                                    C.c_int, C.c_int, _F, _F, _F, _F, _F, _F, _D]
         L.orc_position.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _D, _D,
-                                   _D, C.c_double, C.c_double, _D, _D, _D, _D, _D, _D, _D, _D]
+                                   _D, C.c_double, C.c_double, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.orc_position_loss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _D, _D, _D,
                                         C.c_double, C.c_double, _D]
         L.orc_position_loss.restype = C.c_double
@@ -86,7 +86,7 @@ def amp_std(measured_one: np.ndarray) -> np.ndarray:
 
 def position(V, probe, prop, scan_x, scan_y, amp, *, sigma, dz, binning=1, method=1, adjoint=0):
     """One position in FP64: dict with psi0, far, err, grad (ns slabs, complex),
-    chi0, probe_dir, pos_dir."""
+    chi0, probe_dir, pos_dir, waves (ns+1: psi0, then the wave after each slab)."""
     V = np.ascontiguousarray(V, dtype=np.float64)
     nz, n, _ = V.shape
     ns = 1 if method == 2 else -(-nz // binning)
@@ -95,13 +95,13 @@ def position(V, probe, prop, scan_x, scan_y, amp, *, sigma, dz, binning=1, metho
     am = np.ascontiguousarray(amp, dtype=np.float64)
     out = dict(psi0=np.zeros((n, n), np.complex128), far=np.zeros((n, n), np.complex128),
                grad=np.zeros((ns, n, n), np.complex128), chi0=np.zeros((n, n), np.complex128),
-               probe_dir=np.zeros((n, n), np.complex128))
+               probe_dir=np.zeros((n, n), np.complex128), waves=np.zeros((ns + 1, n, n), np.complex128))
     err = np.zeros(1)
     pd = np.zeros(2)
     c = lambda a: a.view(np.float64).ctypes.data_as(_D)
     rc = lib().orc_position(n, nz, binning, sigma, dz, method, adjoint, _d(V), c(pr), c(pp), float(scan_x),
                             float(scan_y), _d(am), c(out["psi0"]), c(out["far"]), _d(err), c(out["grad"]),
-                            c(out["chi0"]), c(out["probe_dir"]), _d(pd))
+                            c(out["chi0"]), c(out["probe_dir"]), _d(pd), c(out["waves"]))
     assert rc == 0
     out["err"] = float(err[0])
     out["pos_dir"] = pd

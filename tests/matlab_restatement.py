@@ -54,4 +54,5 @@ def step02_step03(V, probe, prop, row, col, meas_centred, sigma, dz, b, pi=np.pi
     de_x = np.gradient(cp, axis=1)   # along dim1 -> "de_probex"
     de_y = np.gradient(cp, axis=0)   # along dim2 -> "de_probey"
     pos = np.array([np.real(np.sum(de_x * bw)), np.real(np.sum(de_y * bw))])
-    return dict(calc=calc, err=err, grad=grad, chi0=bw, probe_dir=probe_dir, pos_dir=pos, psi0=tmp_probe)
+    return dict(calc=calc, err=err, grad=grad, chi0=bw, probe_dir=probe_dir, pos_dir=pos, psi0=tmp_probe,
+                waves=np.stack(save))

@@ -40,6 +40,8 @@ def test_integer_positions_agree(n, nz, b):
     assert abs(o["err"] - ref["err"]) / ref["err"] < 1e-10
     for k in ("psi0", "grad", "chi0", "pos_dir"):
         assert rel_l2(o[k], ref[k]) < 1e-9, k
+    # save_wave_f (STEP02_FORWARD_4D.m:33): the wave after each slab
+    assert rel_l2(o["waves"][1:], ref["waves"]) < 1e-9
     # the shift back by -(s) with pi = 3.1415926 is not exactly integer
     assert rel_l2(o["probe_dir"], ref["probe_dir"]) < 1e-6
 
