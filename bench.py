@@ -522,9 +522,18 @@ def cpu_baseline(args, cfg, spec, meas) -> dict:
     O.batched_tilt(0.5 * spec.volumes[0], spec.probe, spec.prop, spec.scan_x[:k], spec.scan_y[:k], meas[:k],
                    sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
     dt = time.perf_counter() - t0
+    # the reference's sequential semantics (per-position updates) on one core
+    ks = 4
+    t1 = time.perf_counter()
+    O.run_tilt(0.5 * spec.volumes[0], spec.probe, spec.prop, spec.scan_x[:ks], spec.scan_y[:ks], meas[:ks],
+               sigma=spec.sigma, dz=cfg.dx, step=(1e-3, 1e-6, 1e-3), binning=cfg.slice_binning)
+    dt1 = time.perf_counter() - t1
     return {"value": k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
             "sample": f"{k} positions of tilt 0 of the same workload (FP64 C port of the reference path, "
-                      f"OpenMP over positions), {dt:.1f} s"}
+                      f"OpenMP over positions), {dt:.1f} s",
+            "sequential_1core": {"value": ks * ns / dt1, "unit": "slice-propagations/s", "cores": 1,
+                                 "sample": f"run_mset semantics (per-position updates) over {ks} positions of "
+                                           f"tilt 0, FP64 C port, {dt1:.1f} s"}}
 
 
 def run_reference(args):

@@ -1,5 +1,6 @@
 // mset_kernels.cuh -- internal interface between the C-ABI host layer
-// (mset_api.cu) and the fused multislice kernels (mset_kernels.cu).
+// (mset_api.cu) and the fused multislice kernels (mset_kernels_impl.cuh, one
+// translation unit per window size: geo_<N>.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
