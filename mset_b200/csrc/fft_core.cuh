@@ -380,8 +380,13 @@ struct NoPre {
 //   IN  != 0 : finish a scrambled->natural transform of sign IN
 //   op(y, n1, v, pre) : pointwise stage on natural-order real-space values
 //   OUT != 0 : start a natural->scrambled transform of sign OUT
-template <class G, int IN, int OUT, class Pre, class Pf, class Op>
-__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op) {
+struct NoL1 {
+    static constexpr int kLines = 0;
+    __device__ __forceinline__ void operator()(int, int) const {}
+};
+
+template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1 = NoL1>
+__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op, L1 &&l1 = NoL1{}) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
     constexpr int TASKS = O::RPW * R1;
@@ -405,6 +410,14 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
 #pragma unroll 1
     for (int tau = O::lane(); tau < TASKS; tau += 32) {
         const int n1 = tau % R1, y = G::gy(yb, yl0 + tau / R1);
+        if constexpr (std::decay_t<L1>::kLines > 0) {
+            // pull the next iteration's rows of the op's global operands into
+            // L1 (hints: no registers, no scoreboard)
+            constexpr int LN = std::decay_t<L1>::kLines, RI = 32 / R1;
+            const int r0 = yl0 + (tau - O::lane() + 32) / R1;
+            if (r0 < yl0 + O::RPW)
+                for (int q = O::lane(); q < RI * LN; q += 32) l1(G::gy(yb, r0 + q / LN), q % LN);
+        }
         if constexpr (ahead) {
             if (tau + 32 < TASKS) pf(G::gy(yb, yl0 + (tau + 32) / R1), (tau + 32) % R1, nxt);
         } else {
@@ -462,9 +475,34 @@ __device__ __forceinline__ void row_passB(float2 *buf) {
     }
 }
 
+// the R2 twiddles W^(n1 k2) of residue n1 (sign SG): from the transposed
+// table twt[n1][k2] two at a time when TT (R2 even), else from tw[k2][n1]
+template <class G, int SG, bool TT>
+__device__ __forceinline__ void col_twiddles(const float2 *tw, int n1, float2 *w) {
+    constexpr int R1 = G::R1, R2 = G::R2;
+    if constexpr (TT) {
+        const float4 *t4 = reinterpret_cast<const float4 *>(tw + G::N + n1 * R2);
+#pragma unroll
+        for (int m = 0; m < R2 / 2; ++m) {
+            const float4 q = t4[m];
+            w[2 * m] = make_float2(q.x, q.y);
+            w[2 * m + 1] = make_float2(q.z, q.w);
+        }
+        if constexpr (SG > 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) w[k2] = cconj(w[k2]);
+        }
+    } else {
+#pragma unroll
+        for (int k2 = 1; k2 < R2; ++k2) w[k2] = twN<G, SG>(tw, n1, k2);
+    }
+    (void)R1;
+}
+
 // Column pass A.  Task (x, n1) owns rows y = n1 + R1*j.
 //   FWD: natural->scrambled step (DFT then twiddle); else scrambled->natural
-template <class G, int SG, bool FWD>
+//   TT: the transposed twiddle table follows tw (tw + N, [n1][k2])
+template <class G, int SG, bool FWD, bool TT = false>
 __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
@@ -480,13 +518,15 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
             float2 v[R2];
 #pragma unroll
             for (int j = 0; j < R2; ++j) v[j] = p[G::S * j];
+            float2 w[R2];
+            col_twiddles<G, SG, TT>(tw, n1, w);
             if constexpr (FWD) {
                 DFT<R2, SG>::run(v);
 #pragma unroll
-                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], w[k2]);
             } else {
 #pragma unroll
-                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], w[k2]);
                 DFT<R2, SG>::run(v);
             }
 #pragma unroll
@@ -503,13 +543,15 @@ __device__ __forceinline__ void col_passA(float2 *buf, const float2 *tw) {
         float2 v[R2];
 #pragma unroll
         for (int j = 0; j < R2; ++j) v[j] = p[R1 * G::S * j];
+        float2 w[R2];
+        col_twiddles<G, SG, TT>(tw, n1, w);
         if constexpr (FWD) {
             DFT<R2, SG>::run(v);
 #pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], w[k2]);
         } else {
 #pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twN<G, SG>(tw, n1, k2));
+            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], w[k2]);
             DFT<R2, SG>::run(v);
         }
 #pragma unroll

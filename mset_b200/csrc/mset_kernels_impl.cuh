@@ -90,12 +90,36 @@ struct TSPre {
     float2 w[G::R2];  // saved wave
 };
 
+// L1 prefetch of row y of the adjoint's two global operands (transmission
+// slab T, saved wave W), 128-byte line k of 2 * kLPR, issued one task
+// iteration ahead by row_passA_pf.  Used where the rows in flight of every
+// CTA on an SM fit in 64 KB of L1 (+1% per mid pass at n = 128); at n = 256
+// they would take 128 KB and evict each other (-3%).
+template <class G>
+struct L1Rows {
+    static constexpr int kRow = (int)sizeof(float2) * G::N, kLPR = (kRow + 127) / 128;
+    static constexpr long kInFlight = (long)(G::NT / 32) * (32 / G::R1) * 2 * kRow * G::MINB;
+    static constexpr int kLines = (32 % G::R1 == 0 && kInFlight <= 65536) ? 2 * kLPR : 0;
+    const char *T, *W;
+    __device__ __forceinline__ void operator()(int y, int k) const {
+        const char *base = k < kLPR ? T : W;
+        if (!base) return;
+        const int off = min((k < kLPR ? k : k - kLPR) * 128, kRow - (int)sizeof(float2));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(base + (size_t)y * kRow + off));
+    }
+};
+
 // shared-memory layout of the position kernel (float2 units after the field)
 template <class G>
 struct Smem {
-    static constexpr int TW = G::FIELD, E1 = TW + G::N, E2 = E1 + G::N, PY = E2 + G::N, PX = PY + G::N,
-                         END = PX + G::N;
+    // TW: twiddles [k2][n1]; TWT (right after): the same transposed, [n1][k2]
+    static constexpr int TW = G::FIELD, TWT = TW + G::N, E1 = TWT + G::N, E2 = E1 + G::N, PY = E2 + G::N,
+                         PX = PY + G::N, END = PX + G::N;
 };
+// column pass A reads its twiddles from the transposed table two at a time
+// (R2 even): R2/2 16-byte loads per task instead of R2-1 8-byte ones
+template <class G>
+constexpr bool kColTw = G::R2 % 2 == 0;
 
 template <class G, int METHOD, int ADJ, int MODE>
 struct PositionKernel {
@@ -152,6 +176,33 @@ struct PositionKernel {
         return __ldg(a.pscr + (size_t)Ly * N + Lx);
     }
 
+    // v[j] *= P(y0 + j, x) (CONJ: conj(P)) for the R1 rows of a column-pass-B
+    // task.  Separable P: Px(x) is read once and Py two rows at a time
+    // (16-byte loads; y0 is a multiple of R1, the table 16-byte aligned),
+    // 9 shared-memory loads per task instead of 32 (-6% per mid pass)
+    template <bool CONJ>
+    static __device__ __forceinline__ void apply_prop(const LaunchArgs &a, const float2 *py, const float2 *px,
+                                                      int y0, int x, float2 *v) {
+        static_assert(R1 % 2 == 0, "Py is read in pairs");
+        if (a.psep) {
+            const float2 pxv = px[x];
+            const float4 *q4 = reinterpret_cast<const float4 *>(py + y0);
+#pragma unroll
+            for (int m = 0; m < R1 / 2; ++m) {
+                const float4 q = q4[m];
+                const float2 p0 = cmul(make_float2(q.x, q.y), pxv), p1 = cmul(make_float2(q.z, q.w), pxv);
+                v[2 * m] = CONJ ? cmulc(v[2 * m], p0) : cmul(v[2 * m], p0);
+                v[2 * m + 1] = CONJ ? cmulc(v[2 * m + 1], p1) : cmul(v[2 * m + 1], p1);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < R1; ++j) {
+                const float2 p = prop(a, py, px, y0 + j, x);
+                v[j] = CONJ ? cmulc(v[j], p) : cmul(v[j], p);
+            }
+        }
+    }
+
     // forward through slabs s0 .. s1-1 from the checkpointed wave entering s0,
     // storing the wave after slab s at out[s - s0] (mset.cu:157-183)
     static __device__ __noinline__ void recompute(const LaunchArgs &a, const TiltDev &t, int s0, int s1, float2 *buf,
@@ -172,14 +223,13 @@ struct PositionKernel {
         for (int s = s0; s < s1; ++s) {
             row_passB<G, -1>(buf);
             sync_rowcol();
-            col_passA<G, -1, true>(buf, tw);
+            col_passA<G, -1, true, kColTw<G>>(buf, tw);
             sync_cols<G>();
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-#pragma unroll
-                for (int j = 0; j < R1; ++j) v[j] = cmul(v[j], prop(a, py, px, y0 + j, x));
+                apply_prop<false>(a, py, px, y0, x, v);
             });
             sync_cols<G>();
-            col_passA<G, +1, false>(buf, tw);
+            col_passA<G, +1, false, kColTw<G>>(buf, tw);
             sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
@@ -246,8 +296,14 @@ struct PositionKernel {
         // prefetch of the transmission of slab s for a row-pass task
         auto pf_t = [&](int s) {
             return [&, s](int y, int n1, TPre<G> &pre) {
+                if constexpr (MODE == kBatch || MODE == kBatchCk || MODE == kSim) {
+                    const float2 *tr = t.T + (size_t)s * NN + (size_t)y * N + n1;
 #pragma unroll
-                for (int j = 0; j < R2; ++j) pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
+                    for (int j = 0; j < R2; ++j) pre.t[j] = tr[R1 * j];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < R2; ++j) pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
+                }
             };
         };
 
@@ -263,7 +319,7 @@ struct PositionKernel {
             for (int j = 0; j < R1; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
         });
         sync_cols<G>();
-        col_passA<G, -1, false>(buf, tw);
+        col_passA<G, -1, false, kColTw<G>>(buf, tw);
         sync_rowcol();
         row_passB<G, -1>(buf);
         sync_rows();
@@ -283,14 +339,13 @@ struct PositionKernel {
             for (int s = 0; s < ns; ++s) {
                 row_passB<G, -1>(buf);
                 sync_rowcol();
-                col_passA<G, -1, true>(buf, tw);
+                col_passA<G, -1, true, kColTw<G>>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-#pragma unroll
-                    for (int j = 0; j < R1; ++j) v[j] = cmul(v[j], prop(a, py, px, y0 + j, x));
+                    apply_prop<false>(a, py, px, y0, x, v);
                 });
                 sync_cols<G>();
-                col_passA<G, +1, false>(buf, tw);
+                col_passA<G, +1, false, kColTw<G>>(buf, tw);
                 sync_rowcol();
                 row_passB<G, +1>(buf);
                 sync_rows();
@@ -328,7 +383,7 @@ struct PositionKernel {
         // ---- far field, error, residual (mset.cu:186-227) ----
         row_passB<G, -1>(buf);
         sync_rowcol();
-        col_passA<G, -1, true>(buf, tw);
+        col_passA<G, -1, true, kColTw<G>>(buf, tw);
         sync_cols<G>();
         const float *amp = t.amp ? t.amp + (size_t)p * NN : nullptr;
         const unsigned short *ampb = t.ampb ? t.ampb + (size_t)p * NN : nullptr;
@@ -441,7 +496,7 @@ struct PositionKernel {
                                      : (ws == s0 ? save + (size_t)seg * NN : recbuf + (size_t)(ws - s0 - 1) * NN);
             // the saved wave was written long ago (DRAM); have it in L2 by the row pass
             prefetch_l2(wave, (unsigned)(sizeof(float2) * NN));
-            col_passA<G, +1, false>(buf, tw);
+            col_passA<G, +1, false, kColTw<G>>(buf, tw);
             sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
@@ -450,13 +505,31 @@ struct PositionKernel {
             // R2 = 16) exposes its latency and cost 17-22% at n = 256
             auto pf = [&](int y, int n1, TSPre<G> &pre) {
                 const float2 *sv = wave + (size_t)y * N + n1;
+                if constexpr (MODE == kBatch || MODE == kBatchCk) {
+                    // the slab row's address once per task (the descriptor
+                    // lives in shared memory)
+                    const float2 *tr = t.T + (size_t)s * NN + (size_t)y * N + n1;
 #pragma unroll
-                for (int j = 0; j < R2; ++j) {
-                    pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
-                    pre.w[j] = sv[R1 * j];
+                    for (int j = 0; j < R2; ++j) {
+                        pre.t[j] = tr[R1 * j];
+                        pre.w[j] = sv[R1 * j];
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < R2; ++j) {
+                        pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
+                        pre.w[j] = sv[R1 * j];
+                    }
                 }
             };
+            const L1Rows<G> l1{t.T ? reinterpret_cast<const char *>(t.T + (size_t)s * NN) : nullptr,
+                            reinterpret_cast<const char *>(wave)};
             auto gradop = [&](int y, int n1, float2 *v, const TSPre<G> &pre) {
+                // the gradient row's address in a register: an atomic through a
+                // generic pointer could alias the descriptor in shared memory,
+                // which would otherwise be re-read after every atomic
+                double *grow = nullptr;
+                if constexpr (MODE != kSeq && MODE != kStep) grow = t.grad + (size_t)s * NN + (size_t)y * N;
 #pragma unroll
                 for (int j = 0; j < R2; ++j) {
                     const int x = n1 + R1 * j;
@@ -493,25 +566,24 @@ struct PositionKernel {
                             for (int z = z0; z < z1; ++z) V[(size_t)z * NN + (size_t)y * N + x] += du;
                         }
                     } else {
-                        atomicAdd(t.grad + (size_t)s * NN + (size_t)y * N + x, (double)gre);
+                        atomicAdd(grow + x, (double)gre);
                     }
                     v[j] = cmulc(v[j], T);  // chi <- conj(T) chi
                 }
             };
             if (s > 0) {
-                row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop);
+                row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop, l1);
                 sync_rows();
                 row_passB<G, -1>(buf);
                 sync_rowcol();
-                col_passA<G, -1, true>(buf, tw);
+                col_passA<G, -1, true, kColTw<G>>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
-#pragma unroll
-                    for (int j = 0; j < R1; ++j) v[j] = cmulc(v[j], prop(a, py, px, y0 + j, x));
+                    apply_prop<true>(a, py, px, y0, x, v);
                 });
                 sync_cols<G>();
             } else {
-                row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop);
+                row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop, l1);
                 sync_all<G>();
             }
           }
@@ -547,7 +619,7 @@ struct PositionKernel {
         sync_rows();
         row_passB<G, +1>(buf);
         sync_rowcol();
-        col_passA<G, +1, true>(buf, tw);
+        col_passA<G, +1, true, kColTw<G>>(buf, tw);
         sync_cols<G>();
         const float inv = 1.0f / (float)NN;
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
@@ -621,8 +693,10 @@ __device__ __forceinline__ void load_tables(float2 *buf, const LaunchArgs &a) {
     float2 *tw = buf + Smem<G>::TW;
     float2 *py = buf + Smem<G>::PY;
     float2 *px = buf + Smem<G>::PX;
+    float2 *twt = buf + Smem<G>::TWT;
     for (int i = threadIdx.x; i < G::N; i += G::NT) {
         tw[i] = a.twn[i];
+        twt[(i % G::R1) * G::R2 + i / G::R1] = a.twn[i];  // [k2][n1] -> [n1][k2]
         if (a.psep) {
             py[i] = a.psep[i];
             px[i] = a.psep[G::N + i];
