@@ -622,6 +622,10 @@ struct PositionKernel {
         col_passA<G, +1, true, kColTw<G>>(buf, tw);
         sync_cols<G>();
         const float inv = 1.0f / (float)NN;
+        // descriptor fields in registers: the atomics below go through generic
+        // pointers that could alias the shared-memory descriptor
+        float2 *const Qd = t.Q;
+        double *const qacc = t.qacc;
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
             const float2 ex = e2[x];
             const float kx = 2.0f * MSET_REF_PI * shift_grid(G::scr(x), N) / (float)N;
@@ -632,7 +636,7 @@ struct PositionKernel {
                 const float2 d = cscale(cmulc(v[j], fs), inv);
                 if constexpr (ADJ == kEXACT) {
                     // spectral derivative of psi0 w.r.t. the scan coordinates
-                    const float2 qf = cmul(t.Q[li], fs);
+                    const float2 qf = cmul(Qd[li], fs);
                     const float ky = 2.0f * MSET_REF_PI * shift_grid(G::scr(y0 + j), N) / (float)N;
                     // X = Q fs (i kappa); -Re(conj(X) Y)
                     const float2 Xx = make_float2(-qf.y * kx, qf.x * kx);
@@ -641,13 +645,13 @@ struct PositionKernel {
                     pdy -= (double)(Xy.x * v[j].x + Xy.y * v[j].y);
                 }
                 if constexpr (MODE == kSeq || MODE == kStep) {
-                    float2 q = t.Q[li];
+                    float2 q = Qd[li];
                     q.x -= a.step1 * d.x;
                     q.y -= a.step1 * d.y;
-                    t.Q[li] = q;
+                    Qd[li] = q;
                 } else {
-                    atomicAdd(t.qacc + 2 * li, (double)d.x);
-                    atomicAdd(t.qacc + 2 * li + 1, (double)d.y);
+                    atomicAdd(qacc + 2 * li, (double)d.x);
+                    atomicAdd(qacc + 2 * li + 1, (double)d.y);
                 }
             }
         });
