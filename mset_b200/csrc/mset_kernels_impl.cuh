@@ -273,6 +273,11 @@ struct PositionKernel {
         float2 *recbuf = save + (size_t)nseg * NN;
         float2 *park = save + (size_t)(nseg + ck) * NN;
         float *V = t.V;
+        // slab base in a register: generic stores and atomics in the row
+        // passes could alias the shared-memory descriptor, which would then be
+        // re-read once per task
+        const float2 *const Tslab = t.T;
+        double *const gslab = t.grad;
         float sxp, syp;
         if constexpr (MODE == kStep) {
             sxp = a.step_x;
@@ -297,7 +302,7 @@ struct PositionKernel {
         auto pf_t = [&](int s) {
             return [&, s](int y, int n1, TPre<G> &pre) {
                 if constexpr (MODE == kBatch || MODE == kBatchCk || MODE == kSim) {
-                    const float2 *tr = t.T + (size_t)s * NN + (size_t)y * N + n1;
+                    const float2 *tr = Tslab + (size_t)s * NN + (size_t)y * N + n1;
 #pragma unroll
                     for (int j = 0; j < R2; ++j) pre.t[j] = tr[R1 * j];
                 } else {
@@ -508,7 +513,7 @@ struct PositionKernel {
                 if constexpr (MODE == kBatch || MODE == kBatchCk) {
                     // the slab row's address once per task (the descriptor
                     // lives in shared memory)
-                    const float2 *tr = t.T + (size_t)s * NN + (size_t)y * N + n1;
+                    const float2 *tr = Tslab + (size_t)s * NN + (size_t)y * N + n1;
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
                         pre.t[j] = tr[R1 * j];
@@ -529,7 +534,7 @@ struct PositionKernel {
                 // generic pointer could alias the descriptor in shared memory,
                 // which would otherwise be re-read after every atomic
                 double *grow = nullptr;
-                if constexpr (MODE != kSeq && MODE != kStep) grow = t.grad + (size_t)s * NN + (size_t)y * N;
+                if constexpr (MODE != kSeq && MODE != kStep) grow = gslab + (size_t)s * NN + (size_t)y * N;
 #pragma unroll
                 for (int j = 0; j < R2; ++j) {
                     const int x = n1 + R1 * j;
