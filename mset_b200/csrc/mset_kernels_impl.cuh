@@ -90,16 +90,23 @@ struct TSPre {
     float2 w[G::R2];  // saved wave
 };
 
-// L1 prefetch of row y of the adjoint's two global operands (transmission
-// slab T, saved wave W), 128-byte line k of 2 * kLPR, issued one task
-// iteration ahead by row_passA_pf.  Used where the rows in flight of every
-// CTA on an SM fit in 64 KB of L1 (+1% per mid pass at n = 128); at n = 256
-// they would take 128 KB and evict each other (-3%).
-template <class G>
+// L1 prefetch of row y of a row pass A's global operands (transmission slab
+// T, then the adjoint's saved wave W), 128-byte line k, issued one task
+// iteration ahead by row_passA_pf.  Only as many operands as the L1 left
+// beside the shared memory holds with the rows in flight of every CTA on an
+// SM (measured): both operands up to 64 KB in flight (n = 128: +1% per mid
+// pass), the transmission alone up to 56 KB (n = 160: +2.4%, in the adjoint
+// and in the single-buffered forward); none at n = 256 (64 KB per operand:
+// -0.4% with the transmission, -3% with both).
+template <class G, bool FWD = false>
 struct L1Rows {
     static constexpr int kRow = (int)sizeof(float2) * G::N, kLPR = (kRow + 127) / 128;
-    static constexpr long kInFlight = (long)(G::NT / 32) * (32 / G::R1) * 2 * kRow * G::MINB;
-    static constexpr int kLines = (32 % G::R1 == 0 && kInFlight <= 65536) ? 2 * kLPR : 0;
+    static constexpr long kPerOperand = (long)(G::NT / 32) * (32 / G::R1) * kRow * G::MINB;
+    static constexpr bool kFits1 = 32 % G::R1 == 0 && kPerOperand <= 56 * 1024;
+    // forward: the transmission alone, where registers hold no second buffer
+    static constexpr int kOperands = FWD ? (!TPre<G>::kAhead && kFits1 ? 1 : 0)
+                                         : (32 % G::R1 != 0 ? 0 : 2 * kPerOperand <= 65536 ? 2 : kFits1 ? 1 : 0);
+    static constexpr int kLines = kOperands * kLPR;
     const char *T, *W;
     __device__ __forceinline__ void operator()(int y, int k) const {
         const char *base = k < kLPR ? T : W;
@@ -356,6 +363,12 @@ struct PositionKernel {
                 sync_rows();
                 const bool last = s + 1 == ns;
                 const int sn = last ? s : s + 1;
+                // single-buffered transmission prefetch (R2 > 8): pull the next
+                // iteration's rows into L1 as well
+                const L1Rows<G, true> l1f{(Tslab && !last)
+                                        ? reinterpret_cast<const char *>(Tslab + (size_t)sn * NN)
+                                        : nullptr,
+                                    nullptr};
                 row_passA_pf<G, +1, -1, TPre<G>>(
                     buf, tw,
                     [&](int y, int n1, TPre<G> &pre) {
@@ -380,7 +393,8 @@ struct PositionKernel {
 #pragma unroll
                             for (int j = 0; j < R2; ++j) v[j] = cmul(v[j], pre.t[j]);
                         }
-                    });
+                    },
+                    l1f);
                 sync_rows();
             }
         }
