@@ -467,6 +467,7 @@ int mset_upload(mset_session *s, const mset_upload_args *a) {
     s->ready = false;
     s->batch = false;
     s->step_k = -1;
+    s->ckpt = 0;  // the sequential kernels keep every slab's wave
     rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
     if (rc) return rc;
     s->step[0] = a->step_size[0];
