@@ -449,6 +449,20 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
     }
 }
 
+// L1 prefetch of the rows the warp's first row-pass-A iteration will read
+// (issued a pass or two ahead of it; the later iterations are covered one
+// iteration ahead inside row_passA_pf)
+template <class G, class L1>
+__device__ __forceinline__ void l1_first(const L1 &l1) {
+    using O = Own<G>;
+    constexpr int LN = L1::kLines;
+    if constexpr (LN > 0 && 32 % G::R1 == 0) {
+        constexpr int RI = 32 / G::R1;
+        const int yl0 = O::warp() * O::RPW, yb = G::ybase();
+        for (int q = O::lane(); q < RI * LN; q += 32) l1(G::gy(yb, yl0 + q / LN), q % LN);
+    }
+}
+
 template <class G, int IN, int OUT, class Op>
 __device__ __forceinline__ void row_passA(float2 *buf, const float2 *tw, Op &&op) {
     row_passA_pf<G, IN, OUT, NoPre>(
