@@ -14,6 +14,10 @@
  *   'error_sset' (mex_main.cu:33-34,157-184)  mset_error(mode = MSET_MODE_SSET)
  *   clear mset_cuda_kernel (Run_MSET_recon.m:174)   mset_destroy / mset_mex_clear
  *
+ * and the per-position steps of the reference's CPU path (Run_MSET_recon.m:
+ * 136-157): STEP02_FORWARD_4D(_SSET) -> mset_forward_position,
+ * STEP03_BACK(_SSET) -> mset_adjoint_position.
+ *
  * Array layouts are the MEX ones: MATLAB column-major arrays seen as C arrays
  * with the dimensions reversed (mex_tools.hpp:15-24):
  *   RVol         float [nz][n][n]            (MATLAB size n x n x nz)
@@ -149,6 +153,9 @@ int mset_mex_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out,
                  float *error_out);
 int mset_mex_error(int mode, float *error_out);
 int mset_mex_clear(void);
+/* the implicit session (NULL before the first mset_mex_upload), for the
+ * per-position steps and the other session calls from a MEX gateway */
+mset_session *mset_mex_session(void);
 
 /* ---- batched method --------------------------------------------------------
  * Every position of every tilt sees the same volume, probe and positions; the

@@ -42,6 +42,7 @@ SIGNATURES = {
     "mset_mex_run": (C.c_int, [C.c_int, _F, _F, _F, _F, _F]),
     "mset_mex_error": (C.c_int, [C.c_int, _F]),
     "mset_mex_clear": (C.c_int, []),
+    "mset_mex_session": (C.c_void_p, []),
     "mset_batch_setup": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mset_batch_set_tilt": (C.c_int, [C.c_void_p, C.c_int, _F, _F, _F, _F, _F]),
     "mset_batch_set_volume": (C.c_int, [C.c_void_p, C.c_int, _F]),

@@ -722,6 +722,7 @@ int mset_mex_clear(void) {
     g_mex = nullptr;
     return rc;
 }
+mset_session *mset_mex_session(void) { return g_mex; }
 
 // ---- batched method ---------------------------------------------------------
 int mset_batch_setup(mset_session *s, const mset_batch_args *a) {

@@ -53,3 +53,11 @@ def test_create_without_gpu_fails_cleanly():
     rc = lib.mset_create(0, C.byref(h))
     assert rc != 0 and not h.value
     assert b"CUDA" in lib.mset_last_error() or b"device" in lib.mset_last_error()
+
+
+def test_implicit_session_is_null_before_upload():
+    """mset_mex_session: the MEX-style global session does not exist until
+    the first mset_mex_upload (no device work; runs without a GPU)"""
+    import mset_b200
+    lib = mset_b200.load()
+    assert lib.mset_mex_session() is None
