@@ -47,11 +47,18 @@ class Result:
 
 
 class LibraryBackend:
-    """Per-tilt work on the GPU through the C ABI."""
+    """Per-tilt work on the GPU through the C ABI.
 
-    def __init__(self, device: int = 0, vecs=((0, 0, 1), (0, 1, 0), (1, 0, 0))):
+    per_position=False: the CUDA device mode, one fused sequential pass per
+    tilt (mset_run, Run_MSET_recon.m:160-172).  per_position=True: the CPU
+    device modes' loop, STEP02 -> STEP03 -> STEP04 position by position
+    (Run_MSET_recon.m:136-157) through mset_forward_position /
+    mset_adjoint_position; the same updates, one launch per step."""
+
+    def __init__(self, device: int = 0, vecs=((0, 0, 1), (0, 1, 0), (1, 0, 0)), per_position: bool = False):
         self.s = Session(device)
         self.vecs = vecs
+        self.per_position = per_position
 
     def close(self):
         self.s.close()
@@ -64,7 +71,19 @@ class LibraryBackend:
         nsx, nsy = t.n_scan if t.n_scan[0] else (t.scan_x.size, 1)
         self.s.upload(V, t.probe, prop, sigma=sigma, potential_pixelsize=dz, scan_x=t.scan_x, scan_y=t.scan_y,
                       measured=t.measured, step_size=step, slice_binning=binning, n_scan_x=nsx, n_scan_y=nsy)
-        rv, pr, sx, sy, _ = self.s.run(method)
+        if not self.per_position:
+            rv, pr, sx, sy, _ = self.s.run(method)
+            return rv, pr, sx, sy
+        rv = np.array(V, dtype=np.float32, copy=True)
+        sx = np.array(t.scan_x, dtype=np.float32, copy=True)
+        sy = np.array(t.scan_y, dtype=np.float32, copy=True)
+        pr = np.asarray(t.probe, dtype=np.complex64)
+        for k in range(sx.size):
+            self.s.step02(k, sx[k], sy[k], mode=method)
+            g = self.s.step03(mode=method, update_rvol=True)
+            rv += np.float32(step[0]) * g["grad"].real.astype(np.float32)  # STEP04 (:155)
+            sx[k], sy[k] = g["row"], g["col"]
+            pr = g["probe"]
         return rv, pr, sx, sy
 
     def error_tilt(self, V, t: Tilt, prop, *, sigma, dz, binning, method) -> float:

@@ -141,3 +141,24 @@ def test_step_errors(gpu_available):
         s.step03()
         with pytest.raises(mset_b200.MsetError, match="preceding forward_position"):
             s.step03()  # a forward is consumed by one adjoint
+
+
+def test_per_position_backend_equals_fused_backend(gpu_available):
+    """recon.LibraryBackend(per_position=True), the CPU device modes' loop of
+    Run_MSET_recon.m:136-157 on the per-position entry points, updates a tilt
+    as the fused sequential pass does"""
+    from mset_b200 import recon
+    npos = 4
+    c = _case(64, 6, 2, npos, seed=11)
+    step = reasonable_steps(c, MSET_MODE_MSET)
+    t = recon.Tilt(c["probe"], c["sx"], c["sy"], c["meas"], (npos, 1))
+    kw = dict(sigma=c["sigma"], dz=c["dz"], step=step, binning=c["b"], method=MSET_MODE_MSET)
+    outs = []
+    for per_position in (False, True):
+        be = recon.LibraryBackend(per_position=per_position)
+        outs.append(be.run_tilt(c["V"], t, c["prop"], **kw))
+        be.close()
+    (rv0, pr0, sx0, sy0), (rv1, pr1, sx1, sy1) = outs
+    assert rel_l2(rv1 - c["V"], rv0 - c["V"]) < 1e-5
+    assert rel_l2(pr1 - c["probe"], pr0 - c["probe"]) < 1e-5
+    assert rel_l2(np.r_[sx1 - c["sx"], sy1 - c["sy"]], np.r_[sx0 - c["sx"], sy0 - c["sy"]]) < 1e-5
