@@ -145,6 +145,12 @@ int mset_forward_position(mset_session *s, int mode, int k, float row, float col
  * A forward is consumed by one adjoint. */
 int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *resi_in, int update_rvol,
                           float *grad_out, float *probe_out, float *rowcol_out);
+/* the session's current volume and probe, as the per-position loop left them
+ * on the device (Run_MSET_recon.m:136-157 keeps RVol and probe_wave between
+ * positions; here they stay on the GPU, and a caller reads them once per tilt
+ * instead of per position).  rvol_out float [nz][n][n], probe_out float
+ * [n][n][2]; either may be NULL. */
+int mset_read_state(mset_session *s, float *rvol_out, float *probe_out);
 
 /* global-session shims with the MEX's lifetime (one implicit session per
  * process, recreated by every upload, mex_main.cu:13, 56) */
@@ -378,13 +384,17 @@ int mset_tv(mset_session *s, float *vol, int n1, int n2, int n3, double lambda, 
  *   rejected with MSET_E_UNSUPPORTED (n = 128 allows ns up to ~500).
  * Inputs (device): rvol [nz][n][n] float, probe [n][n][2] float, prop2D
  * [n][n][2] centred, scan_x/scan_y [npos], measured [npos][n][n] centred
- * intensities.  Outputs (device), all overwritten: grad [ns][n][n] double,
+ * intensities, finite and non-negative (not checked here: mset_upload refuses
+ * negative, NaN or infinite counts, this pass reads the caller's device
+ * buffer as it is, and such counts give NaN gradients and errors).
+ * Outputs (device), all overwritten: grad [ns][n][n] double,
  * probe_out [n][n][2] double (standard FFT order), posdir [npos][2] double,
  * err [1] double -- the same quantities mset_batch_gradient returns.
  * Work is queued on `stream` (a cudaStream_t, NULL = legacy default stream)
  * and is asynchronous.  The first call on a device resolves the scratch
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  Every call shares the scratch array, so calls whose
+ * array's device address (cudaGetSymbolAddress), and so does the first call
+ * after the device's primary context was reset; make those calls before any
+ * stream capture.  Every call shares the scratch array, so calls whose
  * work overlaps on the GPU (other streams, other host threads) race: order
  * them on one stream. */
 int mset_batch_gradient_noalloc(int device, void *stream, int n, int nz, int slice_binning, int method,

@@ -7,9 +7,10 @@ reference's MEX interface (:mod:`mset_b200.session`), the batched method
 (:mod:`mset_b200.batch`), host physics set-up and the synthetic data
 generator.
 """
-from ._lib import (MSET_ADJOINT_EXACT, MSET_ADJOINT_REF, MSET_MODE_MSET, MSET_MODE_SSET, MsetError,
-                   LIB_PATH, load)
+from ._lib import (MSET_ADJOINT_EXACT, MSET_ADJOINT_REF, MSET_E_ARG, MSET_E_CUDA, MSET_E_NOMEM, MSET_E_STATE,
+                   MSET_E_UNSUPPORTED, MSET_MODE_MSET, MSET_MODE_SSET, MsetError, LIB_PATH, load)
 from .session import Session, mset_cuda_kernel, clear
 
 __all__ = ["Session", "mset_cuda_kernel", "clear", "MsetError", "load", "LIB_PATH",
-           "MSET_MODE_MSET", "MSET_MODE_SSET", "MSET_ADJOINT_REF", "MSET_ADJOINT_EXACT"]
+           "MSET_MODE_MSET", "MSET_MODE_SSET", "MSET_ADJOINT_REF", "MSET_ADJOINT_EXACT", "MSET_E_ARG",
+           "MSET_E_UNSUPPORTED", "MSET_E_CUDA", "MSET_E_STATE", "MSET_E_NOMEM"]

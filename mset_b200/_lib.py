@@ -21,6 +21,12 @@ MSET_MODE_MSET = 1
 MSET_MODE_SSET = 2
 MSET_ADJOINT_REF = 0
 MSET_ADJOINT_EXACT = 1
+# status codes (include/mset_b200.h)
+MSET_E_ARG = -1
+MSET_E_UNSUPPORTED = -2
+MSET_E_CUDA = -3
+MSET_E_STATE = -4
+MSET_E_NOMEM = -5
 
 _F = C.POINTER(C.c_float)
 _D = C.POINTER(C.c_double)
@@ -38,6 +44,7 @@ SIGNATURES = {
     "mset_error": (C.c_int, [C.c_void_p, C.c_int, _F]),
     "mset_forward_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, _F, _F, _F, _F, _F]),
     "mset_adjoint_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F, C.c_int, _F, _F, _F]),
+    "mset_read_state": (C.c_int, [C.c_void_p, _F, _F]),
     "mset_mex_upload": (C.c_int, [C.c_void_p]),
     "mset_mex_run": (C.c_int, [C.c_int, _F, _F, _F, _F, _F]),
     "mset_mex_error": (C.c_int, [C.c_int, _F]),

@@ -515,6 +515,9 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
     if (!rvol_out || !probe_out || !scan_x_out || !scan_y_out) return fail(MSET_E_ARG, "null output array");
     rc = set_device(s);
     if (rc) return rc;
+    // the pass overwrites the saved waves and updates V, probe and positions:
+    // a pending STEP02 can no longer be followed by its STEP03
+    s->step_k = -1;
     rc = ensure_save(s, 1);
     if (rc) return rc;
     rc = refresh_tilt_table(s);
@@ -696,6 +699,22 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
         }
     }
     s->step_k = -1;
+    return 0;
+}
+
+int mset_read_state(mset_session *s, float *rvol_out, float *probe_out) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    if (!s->ready || s->batch) return fail(MSET_E_STATE, "read_state called before upload");
+    int rc = set_device(s);
+    if (rc) return rc;
+    TiltBufs &t = s->tilts[0];
+    const size_t n2 = (size_t)s->n * s->n;
+    if (rvol_out) CK(cudaMemcpyAsync(rvol_out, t.V.p, sizeof(float) * n2 * s->nz, cudaMemcpyDeviceToHost, s->st));
+    if (probe_out) {
+        CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
+        CK(cudaMemcpyAsync(probe_out, s->tmpc.p, sizeof(float2) * n2, cudaMemcpyDeviceToHost, s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
     return 0;
 }
 

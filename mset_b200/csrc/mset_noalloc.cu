@@ -9,6 +9,8 @@
 // spectrum, the probe accumulator, the work counter) lives in one file-scope
 // device array of fixed size, which every GPU that loads the library holds
 // until the process exits.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -27,9 +29,39 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // device address of g_noalloc_scratch, resolved once per device with that
 // device current (the host-side symbol is only a stand-in, not a device
-// address)
+// address), together with the id of the context it was resolved in: after a
+// device reset the module is loaded again in a new primary context and the
+// array may sit elsewhere, so a changed id resolves it again
 std::mutex g_mu;
 void *g_scratch_ptr[64] = {};
+unsigned long long g_scratch_ctx[64] = {};
+
+// id of the context current on this thread (cuCtxGetId through the runtime's
+// driver entry points, so the library needs no link to libcuda); 0 when it
+// cannot be had, and then the address is resolved on every call
+unsigned long long current_context_id() {
+    using PfnGetCurrent = CUresult (*)(CUcontext *);
+    using PfnGetId = CUresult (*)(CUcontext, unsigned long long *);
+    static PfnGetCurrent get_current = nullptr;
+    static PfnGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnGetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnGetId>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
@@ -139,7 +171,8 @@ extern "C" int mset_batch_gradient_noalloc(int device, void *stream, int n, int 
     unsigned char *base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_ptr[device]) {
+        const unsigned long long ctx = current_context_id();
+        if (!g_scratch_ptr[device] || ctx == 0 || ctx != g_scratch_ctx[device]) {
             void *ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess) {
@@ -147,6 +180,7 @@ extern "C" int mset_batch_gradient_noalloc(int device, void *stream, int n, int 
                 return err(MSET_E_CUDA, cudaGetErrorString(e));
             }
             g_scratch_ptr[device] = ptr;
+            g_scratch_ctx[device] = ctx;
         }
         base = static_cast<unsigned char *>(g_scratch_ptr[device]);
     }
@@ -160,8 +194,12 @@ extern "C" int mset_batch_gradient_noalloc(int device, void *stream, int n, int 
     int2 *items = reinterpret_cast<int2 *>(base + off_items);
     float2 *save = reinterpret_cast<float2 *>(base + off_save);
 
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess || sms <= 0) {
+        cudaSetDevice(prev);
+        return err(MSET_E_CUDA, e != cudaSuccess ? cudaGetErrorString(e) : "no multiprocessors reported");
+    }
     const int by_smem = (int)((227 * 1024) / (g->smem + 1024));
     const int per_sm = std::max(1, std::min(std::min(by_smem, 2048 / g->nt), g->minb));
     const int grid = std::max(1, std::min(std::min(slots, sms * per_sm), npos));

@@ -74,16 +74,15 @@ class LibraryBackend:
         if not self.per_position:
             rv, pr, sx, sy, _ = self.s.run(method)
             return rv, pr, sx, sy
-        rv = np.array(V, dtype=np.float32, copy=True)
         sx = np.array(t.scan_x, dtype=np.float32, copy=True)
         sy = np.array(t.scan_y, dtype=np.float32, copy=True)
-        pr = np.asarray(t.probe, dtype=np.complex64)
         for k in range(sx.size):
             self.s.step02(k, sx[k], sy[k], mode=method)
-            g = self.s.step03(mode=method, update_rvol=True)
-            rv += np.float32(step[0]) * g["grad"].real.astype(np.float32)  # STEP04 (:155)
+            # STEP03 and STEP04 (:155) on the device: RVol and the probe stay
+            # there between positions, the scan coordinates come back
+            g = self.s.step03(mode=method, update_rvol=True, want=())
             sx[k], sy[k] = g["row"], g["col"]
-            pr = g["probe"]
+        rv, pr = self.s.read_state()
         return rv, pr, sx, sy
 
     def error_tilt(self, V, t: Tilt, prop, *, sigma, dz, binning, method) -> float:

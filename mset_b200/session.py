@@ -169,22 +169,32 @@ class Session:
         return dict(calc=calc, resi=cplx(resi), waves=cplx(waves), psi0=cplx(psi0), err=float(err[0]))
 
     def step03(self, mode: int = MSET_MODE_MSET, adjoint: int = MSET_ADJOINT_REF, resi=None,
-               update_rvol: bool = False) -> dict:
+               update_rvol: bool = False, want=("grad", "probe")) -> dict:
         """STEP03_BACK(_SSET) after :meth:`step02` (and STEP04 with update_rvol):
         dict with grad ([nz][n][n] complex, slab-replicated), probe (updated)
-        and row, col (updated scan coordinates)"""
+        and row, col (updated scan coordinates); grad / probe only when named
+        in `want` (each is a device-to-host copy)"""
         n = self.n
         ri = None if resi is None else _cplx_f32(resi)
         if ri is not None and ri.shape != (n, n, 2):
             raise ValueError("resi must be n x n complex")
-        grad = np.empty((self.nz, n, n, 2), np.float32)
-        probe = np.empty((n, n, 2), np.float32)
+        grad = np.empty((self.nz, n, n, 2), np.float32) if "grad" in want else None
+        probe = np.empty((n, n, 2), np.float32) if "probe" in want else None
         rc = np.zeros(2, np.float32)
         check("mset_adjoint_position",
               self._lib.mset_adjoint_position(self._h, int(mode), int(adjoint), fptr(ri) if ri is not None else None,
                                               int(bool(update_rvol)), fptr(grad), fptr(probe), fptr(rc)))
-        cplx = lambda a: a.view(np.complex64)[..., 0]
+        cplx = lambda a: None if a is None else a.view(np.complex64)[..., 0]
         return dict(grad=cplx(grad), probe=cplx(probe), row=float(rc[0]), col=float(rc[1]))
+
+    def read_state(self):
+        """(rvol [nz][n][n] float32, probe [n][n] complex64): the session's
+        volume and probe as the per-position steps left them on the device"""
+        n = self.n
+        rv = np.empty((self.nz, n, n), np.float32)
+        probe = np.empty((n, n, 2), np.float32)
+        check("mset_read_state", self._lib.mset_read_state(self._h, fptr(rv), fptr(probe)))
+        return rv, probe.view(np.complex64)[..., 0]
 
     def _ns(self) -> int:
         b = max(1, min(self._binning, self.nz))

@@ -1,0 +1,197 @@
+"""GPU parity at the geometries the benchmark runs, against the FP64 oracle.
+
+The small parity cases (tests/test_gpu_parity.py) use at most 9 slabs; FP32
+error accumulates over the 64 slabs of the mid workload and the 96 slabs of
+the large one, so the library is compared here with the oracle on the real
+synthetic specimens of those workloads (synth.CONFIGS), on sampled positions
+spread over each scan:
+
+* mid: 128^2 window, 128^3 volume, 64 slabs x 2 voxels, 16 positions of the
+  -60 deg tilt;
+* large: 256^2 window (one field over a 4-CTA cluster), 256x256x192 volume,
+  96 slabs x 2 voxels, 4 positions of the -70 deg tilt, BF16 counts;
+* uneven_160: 160^2 window, 96^3 volume padded to 160^2, 96 slabs x 1 voxel,
+  8 positions of the -70 deg tilt;
+* the sequential pass (run_mset semantics, per-position updates of volume,
+  probe and scan positions) at the mid geometry.
+
+Measured intensities: the library's own forward model at the true volume plus
+seeded Poisson noise at the configuration's dose; both implementations then
+take the gradient at half the true potential (a mid-reconstruction state) from
+the same bytes.  Tolerances are relative L2 against the FP64 oracle.
+
+What FP32 propagation can resolve here.  These specimens are weak phase
+objects (sigma * dz * sum V ~ 2.5 mrad through the whole column), so the
+gradient lives in the dark field of the far field, ~1e-3 of the bright-field
+amplitude, while every FP32 transform leaves rounding noise ~1e-7 of the
+bright field spread over all pixels, and ~100 slabs x 4 transforms add it
+up.  Measured on one B200 (per position, volume gradient vs the FP64 oracle):
+
+  geometry      this library      the reference's own FP32 CUDA (cuFFT)
+  mid 128^2     3e-5 - 6e-5       7e-5 - 5.7e-4
+  uneven_160    1.2e-4 - 4.3e-4   1.1e-3 - 1.5e-3
+  uneven_96b    2.8e-4 - 4.9e-4   1.1e-3 - 3.0e-3
+
+so the volume gradient, probe direction and error are held to 1e-4 at the mid
+and large geometries, and at 160^2 / 96 slabs of 1 voxel to 5e-4 and to no
+more than the reference's own deviation on the same inputs (measured live
+when oracle/_ref is built).  Scan-position directions are sums of N^2
+products with cancellation factors of 1e3 and more; with the reference formula
+(finite differences of the shifted probe) FP32 gives 1e-4 - 1.5e-3, with the
+exact spectral derivative (weighted by the spatial frequency, where the
+back-propagated field is least precise) 2e-2 - 1.2e-1 over 64-96 slabs; the
+bounds in POS_TOL say so.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from mset_b200 import MSET_ADJOINT_EXACT, MSET_ADJOINT_REF, MSET_MODE_MSET, Session, synth
+from mset_b200.batch import BatchSession
+from oracle import oracle as O, refharness
+from tests.helpers import reasonable_steps, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+# volume gradient / probe direction / error, per geometry (see above)
+GRAD_TOL = {"mid": 1e-4, "large": 1e-4, "uneven_160": 5e-4}
+# scan-position directions: (reference formula, exact formula) per window
+POS_TOL = {128: (1e-3, 0.1), 160: (3e-3, 0.15), 256: (1e-3, 0.25)}
+
+GEOMETRIES = {
+    # name: (config, tilts generated, tilt used, positions sampled, BF16 counts)
+    "mid": (synth.CONFIGS["mid"], 3, 0, 16, False),
+    "large": (synth.CONFIGS["large"], 3, 0, 4, True),
+    "uneven_160": (synth.UNEVEN[3], 3, 0, 8, False),
+}
+
+
+def _problem(name):
+    cfg, ntilt, j, k, bf16 = GEOMETRIES[name]
+    cfg = dataclasses.replace(cfg, n_tilts=ntilt)
+    spec = synth.make_specimen(cfg)
+    idx = np.linspace(0, spec.scan_x.size - 1, k).round().astype(int)
+    sx, sy = spec.scan_x[idx], spec.scan_y[idx]
+    vt = spec.volumes[j]
+    n = cfg.window
+    # data: the library's forward model at the true volume, seeded Poisson counts
+    bs = BatchSession(n=n, nz=vt.shape[0], npos=[k], prop=spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx,
+                      slice_binning=cfg.slice_binning)
+    bs.set_tilt(0, probe=spec.probe, scan_x=sx, scan_y=sy, measured=np.zeros((k, n, n), np.float32), volume=vt)
+    inten = bs.simulate()
+    bs.close()
+    meas = synth.poisson(inten, cfg.seed + 1000)
+    return dict(cfg=cfg, spec=spec, sx=sx, sy=sy, V=(0.5 * vt).astype(np.float32), meas=meas, bf16=bf16)
+
+
+def _bf16(a):
+    """float32 -> BF16 (round to nearest even) -> float32"""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32)
+
+
+@pytest.fixture(scope="module", params=list(GEOMETRIES))
+def geometry(request, gpu_available):
+    return request.param, _problem(request.param)
+
+
+@pytest.mark.parametrize("admode", [MSET_ADJOINT_REF, MSET_ADJOINT_EXACT], ids=["ref", "exact"])
+def test_batched_pass_matches_oracle_at_benchmark_geometry(geometry, admode):
+    name, p = geometry
+    cfg, spec = p["cfg"], p["spec"]
+    n, k = cfg.window, p["sx"].size
+    bs = BatchSession(n=n, nz=p["V"].shape[0], npos=[k], prop=spec.prop, sigma=spec.sigma,
+                      potential_pixelsize=cfg.dx, slice_binning=cfg.slice_binning, method=MSET_MODE_MSET,
+                      adjoint=admode)
+    if p["bf16"]:
+        bs.set_amplitude_bf16(True)  # Poisson counts <= 256 are exact in BF16
+    bs.set_tilt(0, probe=spec.probe, scan_x=p["sx"], scan_y=p["sy"], measured=p["meas"], volume=p["V"])
+    out = bs.gradient()
+    bs.close()
+    meas = p["meas"]
+    if p["bf16"]:
+        meas = _bf16(meas)  # the counts the library holds (BF16 rounds integers above 256)
+    g, pa, pd, e = O.batched_tilt(p["V"], spec.probe, spec.prop, p["sx"], p["sy"], meas, sigma=spec.sigma,
+                                  dz=cfg.dx, binning=cfg.slice_binning, adjoint=admode)
+    errs = {"grad": rel_l2(out["grad"][0], g), "probe": rel_l2(np.fft.fft2(out["probe"][0]), pa),
+            "err": abs(out["err"][0] - e) / e, "posdir": rel_l2(out["posdir"], pd)}
+    print(name, admode, {q: f"{v:.2e}" for q, v in errs.items()})
+    tol = GRAD_TOL[name]
+    assert errs["grad"] < tol
+    assert errs["probe"] < tol
+    assert errs["err"] < tol
+    assert errs["posdir"] < POS_TOL[n][admode]
+
+
+def test_sequential_pass_matches_oracle_at_mid_geometry(gpu_available):
+    """run_mset (per-position updates of volume, probe and positions) over 6
+    positions of the mid workload, 64 slabs; the changes the pass makes
+    against the FP64 oracle's sequential pass"""
+    p = _problem("mid")
+    cfg, spec = p["cfg"], p["spec"]
+    k = 6
+    sx, sy, meas = p["sx"][:k], p["sy"][:k], p["meas"][:k]
+    c = dict(V=p["V"], probe=spec.probe, prop=spec.prop, sx=sx, sy=sy, meas=meas, sigma=spec.sigma, dz=cfg.dx,
+             b=cfg.slice_binning)
+    step = reasonable_steps(c, 1, 0, frac=(0.02, 0.005, 0.05))
+    rv_o, pr_o, sx_o, sy_o, err_o = O.run_tilt(p["V"], spec.probe, spec.prop, sx, sy, meas, sigma=spec.sigma,
+                                               dz=cfg.dx, step=step, binning=cfg.slice_binning)
+    with Session() as s:
+        s.upload(p["V"], spec.probe, spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx, scan_x=sx, scan_y=sy,
+                 measured=meas, step_size=step, slice_binning=cfg.slice_binning)
+        rv, pr, sxo, syo, err = s.run(MSET_MODE_MSET)
+    errs = {"rvol": rel_l2(rv - p["V"], rv_o - p["V"]), "probe": rel_l2(pr - spec.probe, pr_o - spec.probe),
+            "pos": rel_l2(np.r_[sxo - sx, syo - sy], np.r_[sx_o - sx, sy_o - sy])}
+    n2 = cfg.window ** 2
+    errs["err"] = abs(err - err_o / k / n2) / (err_o / k / n2)  # mex_main.cu:150
+    print("sequential mid", {q: f"{v:.2e}" for q, v in errs.items()})
+    assert errs["rvol"] < TOL
+    assert errs["probe"] < TOL
+    assert errs["pos"] < POS_TOL[128][0]
+    assert errs["err"] < TOL
+
+
+@pytest.mark.skipif(not refharness.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["uneven_160", "uneven_96b"])
+def test_weak_phase_gradient_is_closer_to_fp64_than_the_reference(gpu_available, name):
+    """Per position, the volume gradient of this library and of the
+    reference's own CUDA module (src/CUDA/mset.cu with cuFFT, compiled
+    unchanged), both FP32, against the FP64 oracle, on the 96-slab weak-phase
+    geometries where FP32 cannot reach 1e-4.  The reference's gradient is read
+    from a one-position run_mset with a large object step and no probe or
+    position step: RVol_out - RVol_in = step0 Re(g), slab-replicated
+    (mset.cu:265-284)."""
+    cfg = {"uneven_160": synth.UNEVEN[3], "uneven_96b": synth.UNEVEN[5]}[name]
+    cfg = dataclasses.replace(cfg, n_tilts=3)
+    spec = synth.make_specimen(cfg)
+    k = 4
+    idx = np.linspace(0, spec.scan_x.size - 1, k).round().astype(int)
+    sx, sy = spec.scan_x[idx], spec.scan_y[idx]
+    vt = spec.volumes[0]
+    n, b = cfg.window, cfg.slice_binning
+    bs = BatchSession(n=n, nz=vt.shape[0], npos=[k], prop=spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx,
+                      slice_binning=b)
+    bs.set_tilt(0, probe=spec.probe, scan_x=sx, scan_y=sy, measured=np.zeros((k, n, n), np.float32), volume=vt)
+    meas = synth.poisson(bs.simulate(), cfg.seed + 1000)
+    bs.close()
+    V = (0.5 * vt).astype(np.float32)
+    ns = -(-V.shape[0] // b)
+    for p in range(k):
+        one = dict(scan_x=sx[p:p + 1], scan_y=sy[p:p + 1], measured=meas[p:p + 1])
+        g, _, _, _ = O.batched_tilt(V, spec.probe, spec.prop, one["scan_x"], one["scan_y"], one["measured"],
+                                    sigma=spec.sigma, dz=cfg.dx, binning=b)
+        s0 = float(np.abs(V).max() / np.abs(g).max())  # moves V by ~its own size: no FP32 loss in the sum
+        r = refharness.RefSession()
+        r.upload(V, spec.probe, spec.prop, sigma=spec.sigma, dz=cfg.dx, step=(s0, 0, 0), binning=b, **one)
+        g_ref = ((r.run(1)[0].astype(np.float64) - V) / s0)[::b][:ns]
+        bs = BatchSession(n=n, nz=V.shape[0], npos=[1], prop=spec.prop, sigma=spec.sigma,
+                          potential_pixelsize=cfg.dx, slice_binning=b)
+        bs.set_tilt(0, probe=spec.probe, volume=V, **one)
+        g_lib = bs.gradient(want=("grad",))["grad"][0]
+        bs.close()
+        e_lib, e_ref = rel_l2(g_lib, g), rel_l2(g_ref, g)
+        print(name, p, f"library {e_lib:.2e} reference {e_ref:.2e}")
+        assert e_lib < 1e-3
+        assert e_lib < e_ref

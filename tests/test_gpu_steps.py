@@ -91,6 +91,10 @@ def test_step_loop_equals_sequential_run(gpu_available, method):
             rows[k], cols[k] = g["row"], g["col"]
             e += f["err"]
         probe = g["probe"]
+        # the volume and probe the device holds after the loop
+        rv_dev, pr_dev = s.read_state()
+    assert rel_l2(rv_dev - c["V"], rv - c["V"]) < 1e-5
+    assert rel_l2(pr_dev, probe) < 1e-6
     assert rel_l2(V - c["V"], rv - c["V"]) < 1e-5
     assert rel_l2(probe - c["probe"], pr - c["probe"]) < 1e-5
     assert rel_l2(np.r_[rows - c["sx"], cols - c["sy"]], np.r_[sx - c["sx"], sy - c["sy"]]) < 1e-5
@@ -141,6 +145,13 @@ def test_step_errors(gpu_available):
         s.step03()
         with pytest.raises(mset_b200.MsetError, match="preceding forward_position"):
             s.step03()  # a forward is consumed by one adjoint
+        # a sequential pass between STEP02 and STEP03 overwrites the saved
+        # waves and the volume / probe / positions the forward used
+        s.step02(0, 12.0, 12.0)
+        s.run(MSET_MODE_MSET)
+        with pytest.raises(mset_b200.MsetError, match="preceding forward_position") as ei:
+            s.step03()
+        assert ei.value.code == mset_b200.MSET_E_STATE
 
 
 def test_per_position_backend_equals_fused_backend(gpu_available):
