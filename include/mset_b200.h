@@ -249,7 +249,8 @@ typedef struct {
     double us_per_position; /* measured device time per position at this shape */
     double save_bytes;      /* saved-wave storage at this shape */
     int32_t threads;        /* threads per CTA of the chosen kernel shape */
-    int32_t reserved;
+    int32_t staged;         /* 1: the shape stages the adjoint's saved-wave rows in
+                               shared memory by bulk copies (TMA engine) */
 } mset_tune_result;
 int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out);
 /* compiled kernel shapes of window size n (threads per CTA and register

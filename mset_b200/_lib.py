@@ -162,7 +162,7 @@ class TuneResult(C.Structure):
         ("us_per_position", C.c_double),
         ("save_bytes", C.c_double),
         ("threads", C.c_int32),
-        ("reserved", C.c_int32),
+        ("staged", C.c_int32),
     ]
 
     def as_dict(self):

@@ -100,12 +100,23 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk(a)), "l"(pk(b)));
     return upk(r);
 }
+// Complex multiply with the packed multiply and fused multiply-add of sm_100
+// (mul.f32x2 / fma.f32x2): a*b = (a.x b.x, a.y b.x) + (a.y, a.x) (-b.y, b.y),
+// two issue slots instead of four (the FP32 pipe does the same work).
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+    unsigned long long t, r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(pk(a)), "l"(pk(make_float2(b.x, b.x))));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(make_float2(a.y, a.x))), "l"(pk(make_float2(-b.y, b.y))),
+        "l"(t));
+    return upk(r);
 }
-// a * conj(b)
+// a * conj(b) = (a.x b.x, a.y b.x) + (a.y, a.x) (b.y, -b.y)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+    unsigned long long t, r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(pk(a)), "l"(pk(make_float2(b.x, b.x))));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(make_float2(a.y, a.x))), "l"(pk(make_float2(b.y, -b.y))),
+        "l"(t));
+    return upk(r);
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
@@ -243,9 +254,10 @@ struct DFT {
 // ---------------------------------------------------------------------------
 // geometry of one N x N field in shared memory
 // ---------------------------------------------------------------------------
-template <int N_, int R1_, int NT_, int MINB_ = 1>
+template <int N_, int R1_, int NT_, int MINB_ = 1, bool STAGE_ = false>
 struct Geo {
     static constexpr int MINB = MINB_;  // CTAs per SM the register budget is sized for
+    static constexpr bool STAGE = STAGE_;  // adjoint's saved-wave rows staged by bulk copies
     static constexpr int N = N_;
     static constexpr int R1 = R1_;
     static constexpr int R2 = N_ / R1_;
@@ -385,11 +397,22 @@ struct NoL1 {
     __device__ __forceinline__ void operator()(int, int) const {}
 };
 
-template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1 = NoL1>
-__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op, L1 &&l1 = NoL1{}) {
+// No operand staged in shared memory (see RowStage in mset_kernels_impl.cuh):
+// the op takes (y, n1, v, pre).
+struct NoStage {
+    static constexpr bool kOn = false;
+    __device__ __forceinline__ void wait(int) const {}
+    __device__ __forceinline__ void refill(int) const {}
+    __device__ __forceinline__ const float2 *task(int, int) const { return nullptr; }
+};
+
+template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1 = NoL1, class ST = NoStage>
+__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op, L1 &&l1 = NoL1{},
+                                             const ST &st = ST{}) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
     constexpr int TASKS = O::RPW * R1;
+    static_assert(!ST::kOn || TASKS % 32 == 0, "a staged operand needs whole warp iterations");
     const int yl0 = O::warp() * O::RPW;  // first local row of the warp
     const int yb = G::ybase();           // local row -> row of the field (pf / op)
     // Pre::kAhead: issue the next task's global loads while the current task
@@ -437,7 +460,16 @@ __device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &
             for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, IN>{}));
             DFT<R2, IN>::run(v);
         }
-        op(y, n1, v, pre);
+        if constexpr (ST::kOn) {
+            // the staged operand rows of this warp iteration: wait for their
+            // bulk copy, hand the task its row, refill the stage afterwards
+            const int it = (tau - O::lane()) >> 5;
+            st.wait(it);
+            op(y, n1, v, pre, st.task(it, O::lane()));
+            st.refill(it);
+        } else {
+            op(y, n1, v, pre);
+        }
         if constexpr (OUT != 0) {
             DFT<R2, OUT>::run(v);
 #pragma unroll

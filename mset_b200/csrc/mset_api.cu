@@ -121,6 +121,7 @@ struct mset_session {
     DevBuf<TiltDev> d_tilts;
     DevBuf<int2> items;
     DevBuf<unsigned> counter;
+    DevBuf<unsigned> fault;  // [1] set by a position kernel whose bounded wait gave up
     DevBuf<float> inten;
     int save_slots = 0;
     int ckpt = 0;  // checkpoint interval of the batched pass (0: keep every wave)
@@ -365,7 +366,23 @@ LaunchArgs base_args(mset_session *s) {
     a.seq_tilt = 0;
     a.ckpt = s->ckpt;
     a.slots = save_slots(s->ns, s->ckpt);
+    a.fault = s->fault.p;
     return a;
+}
+
+// The position kernel waits, with a bound, for the bulk copies that stage
+// its operands in shared memory; a wait that gave up sets the session's
+// fault word.  Read (and clear) it where a call hands results back.
+int take_fault(mset_session *s) {
+    if (!s->fault.p) return 0;
+    unsigned f = 0;
+    CK(cudaMemcpyAsync(&f, s->fault.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (!f) return 0;
+    CK(cudaMemsetAsync(s->fault.p, 0, sizeof(unsigned), s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return fail(MSET_E_CUDA, "a bulk copy into shared memory did not complete within the position kernel's "
+                             "bounded wait; the results of this call are invalid");
 }
 
 int effective_mode(const mset_session *s, int method, int mode) {
@@ -428,6 +445,8 @@ int mset_create(int device, mset_session **out) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
+    if (e == cudaSuccess) e = s->fault.ensure(1);
+    if (e == cudaSuccess) e = cudaMemset(s->fault.p, 0, sizeof(unsigned));
     if (e != cudaSuccess) {
         delete s;
         return cuda_fail(e, "session setup");
@@ -538,7 +557,7 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
     CK(cudaMemcpyAsync(&e, s->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if (error_out) *error_out = (float)(e / ((double)s->nsx * s->nsy) / (double)n2);  // mex_main.cu:150
-    return 0;
+    return take_fault(s);
 }
 
 int mset_run(mset_session *s, int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out,
@@ -699,7 +718,7 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
         }
     }
     s->step_k = -1;
-    return 0;
+    return take_fault(s);
 }
 
 int mset_read_state(mset_session *s, float *rvol_out, float *probe_out) {
@@ -911,7 +930,7 @@ int mset_batch_read_gradient(mset_session *s, double *grad_out, double *probe_ou
     }
     if (err_out) CK(cudaMemcpyAsync(err_out, s->err.p, sizeof(double) * J, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    return 0;
+    return take_fault(s);
 }
 
 int mset_batch_error(mset_session *s, double *err_out) {
@@ -992,7 +1011,7 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_pass = ms / reps;
-    return 0;
+    return take_fault(s);
 }
 
 // ---- Fourier-shear rotation -------------------------------------------------
@@ -1275,7 +1294,7 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
     if (tv_err_out && niter)
         CK(cudaMemcpyAsync(tv_err_out, s->tv_hist.p, sizeof(double) * niter, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    return 0;
+    return take_fault(s);
 }
 
 // TV / TV-FISTA of rec / max(rec), rescaled by max(rec) (Run_MSET_recon.m:267-270)
@@ -1416,7 +1435,7 @@ int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, dou
     }
     CK(cudaStreamSynchronize(s->st));
     if (iters_out) *iters_out = done;
-    return 0;
+    return take_fault(s);
 }
 
 int mset_batch_iterate_phase(mset_session *s, int phase, int use_graph) {
@@ -1489,7 +1508,7 @@ int mset_batch_iterate_time(mset_session *s, int niter, double *ms_per_iter) {
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_iter = ms / niter;
-    return 0;
+    return take_fault(s);
 }
 
 int mset_batch_set_amplitude_bf16(mset_session *s, int on) {
@@ -1649,6 +1668,7 @@ int tune_session(mset_session *s, double budget, mset_tune_result *out) {
         out->us_per_position = best_us;
         out->save_bytes = best_bytes;
         out->threads = s->plan.nt;
+    out->staged = s->plan.staged;
     }
     return 0;
 }
@@ -1822,6 +1842,7 @@ int mset_batch_get_tune(mset_session *s, mset_tune_result *out) {
     out->us_per_position = s->tuned_us_per_pos;
     out->save_bytes = save_bytes(s, grid, s->ckpt);
     out->threads = s->plan.nt;
+    out->staged = s->plan.staged;
     return 0;
 }
 
@@ -1923,6 +1944,8 @@ int mset_group_gradient(mset_group *g, int use_graph) {
     rc = group_launch(g, grids, use_graph != 0);
     if (rc) return rc;
     CK(cudaStreamSynchronize(g->st));
+    for (mset_session *m : g->m)
+        if ((rc = take_fault(m)) != 0) return rc;
     return 0;
 }
 
@@ -1943,6 +1966,8 @@ int mset_group_time(mset_group *g, int reps, int use_graph, double *ms_per_pass)
     float t = 0;
     CK(cudaEventElapsedTime(&t, g->ev0, g->ev1));
     *ms_per_pass = t / reps;
+    for (mset_session *m : g->m)
+        if ((rc = take_fault(m)) != 0) return rc;
     return 0;
 }
 

@@ -8,7 +8,7 @@ namespace mset {
 
 // every compiled geometry; the first entry of a window size is its default,
 // the others are alternative thread shapes the autotuner may pick
-#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(64v2) X(96) X(96v2) X(128) X(128v2) X(160) X(160v2) X(256) X(256v2)
+#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(64v2) X(96) X(96v2) X(128) X(128v2) X(128s) X(160) X(160v2) X(256) X(256v2)
 #define X(N_) extern const GeoOps kGeo##N_;
 MSET_GEOS(X)
 #undef X
@@ -38,6 +38,7 @@ bool plan_for(int n, Plan *p, int variant) {
     p->r1 = g->r1;
     p->nt = g->nt;
     p->cl = g->cl;
+    p->staged = g->staged;
     p->max_clusters = 0;
     p->smem = g->smem;
     p->ctas_per_sm = 0;

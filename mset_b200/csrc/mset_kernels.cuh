@@ -64,6 +64,7 @@ struct LaunchArgs {
     float2 *step_grad;      // [ns][n][n] complex gradient i conj(T) conj(psi) chi (STEP03)
     float *step_pos;        // [2] updated scan coordinates (STEP03)
     double *step_err;       // [1] += sum over pixels of (A - M)^2 (STEP02; zeroed by the host)
+    unsigned *fault;        // [1] set by a kernel whose bounded wait gave up (may be null)
 };
 
 // saved-wave slots a CTA needs for ns slabs with checkpoint interval k
@@ -78,6 +79,7 @@ struct GeoOps {
     int n, r1, nt;
     int cl;  // CTAs per field (thread-block cluster size; 1: one CTA per position)
     size_t smem;
+    int staged;  // the adjoint's saved-wave rows are staged in shared memory by bulk copies
     int (*max_clusters)();  // clusters resident at once (cluster geometries)
     int (*positions)(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st);
     int (*prep_amp)(const float *meas_centred, float *amp_scr, long npos, cudaStream_t st);
@@ -90,6 +92,7 @@ struct GeoOps {
 struct Plan {
     int n, r1, nt;
     int cl;
+    int staged;        // GeoOps::staged
     int max_clusters;  // cl > 1: clusters resident at once (0: unknown)
     size_t smem;
     int ctas_per_sm;

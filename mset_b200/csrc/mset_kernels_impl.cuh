@@ -84,6 +84,11 @@ struct TPre {
     float2 t[G::R2];  // transmission of the task's elements
 };
 template <class G>
+struct T1Pre {
+    static constexpr bool kAhead = false;  // loaded just before the task's shared-memory reads
+    float2 t[G::R2];
+};
+template <class G>
 struct TSPre {
     static constexpr bool kAhead = false;  // two operands: no room for a second buffer
     float2 t[G::R2];  // transmission
@@ -98,14 +103,17 @@ struct TSPre {
 // pass), the transmission alone up to 56 KB (n = 160: +2.4%, in the adjoint
 // and in the single-buffered forward); none at n = 256 (64 KB per operand:
 // -0.4% with the transmission, -3% with both).
-template <class G, bool FWD = false>
+template <class G, bool FWD = false, bool TONLY = false>
 struct L1Rows {
     static constexpr int kRow = (int)sizeof(float2) * G::N, kLPR = (kRow + 127) / 128;
     static constexpr long kPerOperand = (long)(G::NT / 32) * (32 / G::R1) * kRow * G::MINB;
     static constexpr bool kFits1 = 32 % G::R1 == 0 && kPerOperand <= 56 * 1024;
-    // forward: the transmission alone, where registers hold no second buffer
+    // forward: the transmission alone, where registers hold no second buffer;
+    // TONLY: the adjoint's transmission alone (its saved wave is staged in
+    // shared memory by bulk copies)
     static constexpr int kOperands = FWD ? (!TPre<G>::kAhead && kFits1 ? 1 : 0)
-                                         : (32 % G::R1 != 0 ? 0 : 2 * kPerOperand <= 65536 ? 2 : kFits1 ? 1 : 0);
+                                   : TONLY ? (kFits1 ? 1 : 0)
+                                           : (32 % G::R1 != 0 ? 0 : 2 * kPerOperand <= 65536 ? 2 : kFits1 ? 1 : 0);
     static constexpr int kLines = kOperands * kLPR;
     const char *T, *W;
     __device__ __forceinline__ void operator()(int y, int k) const {
@@ -131,12 +139,108 @@ struct L1FirstT {
     }
 };
 
+// Staging of the adjoint's saved-wave rows in shared memory by bulk copies
+// of the TMA engine (cp.async.bulk global -> shared, completion counted on an
+// mbarrier).  Row pass A of a slab's adjoint reads, per warp iteration, kRows
+// whole rows of the wave saved in the forward; each warp owns two stages of
+// kRows rows.  The first two iterations' rows are requested at the top of the
+// slab, two passes before they are read; iteration it + 2's rows as soon as
+// iteration it has read its stage.  The rows then cost a shared-memory load
+// instead of a global load held in registers across the task (16 registers
+// fewer at n = 128, and no spills).  Single-CTA fields only (a bulk copy of
+// whole contiguous rows), in the geometries compiled with STAGE (n = 128:
+// 2 stages x 2 rows x 1 KB x 16 warps = 64 KB beside the 139 KB field).
+// Measured on the mid workload it trades the global-load waits for
+// shared-memory queueing (long-scoreboard stalls per issue 1.49 -> 0.72,
+// MIO-throttle 0.74 -> 1.19) and is not faster than the register path, so it
+// is a variant the autotuner times, not the default.
+template <class G>
+struct StageCfg {
+    static constexpr int kRows = 32 % G::R1 == 0 ? 32 / G::R1 : 1;  // rows of one warp iteration
+    static constexpr int kIters = Own<G>::RPW * G::R1 / 32;          // warp iterations per row pass
+    static constexpr unsigned kBytes = (unsigned)(kRows * G::N * sizeof(float2));
+    static constexpr int kWarps = G::NT / 32;
+    static constexpr bool kOn = G::STAGE && G::CL == 1 && 32 % G::R1 == 0 && Own<G>::RPW % kRows == 0 &&
+                                kIters >= 2 && kIters % 2 == 0 && G::R2 <= 8;
+    static constexpr int kStageF2 = kOn ? 2 * kRows * G::N * kWarps : 0;  // stages, float2 units
+    static constexpr int kBarF2 = kOn ? 2 * kWarps : 0;                    // one mbarrier (8 B) per stage
+};
+
+// bounded wait on an mbarrier phase: false if it did not complete within
+// ~4M polls (with back-off), which no bulk copy of a few KB can take
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+template <class G>
+struct RowStage {
+    using C = StageCfg<G>;
+    static constexpr bool kOn = true;
+    float2 *base;        // this warp's two stages [2][kRows][N]
+    uint32_t bar;        // shared address of this warp's two mbarriers
+    const float2 *src;   // the operand [N][N] in global memory
+    int yl0;             // first row of the warp
+    unsigned phase;      // stage completions before this pass, per stage
+    unsigned *fault;     // set when a wait gave up (may be null)
+
+    // request the rows of warp iteration it (lane 0; the stage is free)
+    __device__ __forceinline__ void issue(int it) const {
+        const float2 *g = src + (size_t)(yl0 + it * C::kRows) * G::N;
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(base + (it & 1) * C::kRows * G::N);
+        const uint32_t b = bar + 8u * (uint32_t)(it & 1);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(C::kBytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                     "l"(g), "r"(C::kBytes), "r"(b)
+                     : "memory");
+    }
+    // the first two iterations, at the top of the slab
+    __device__ __forceinline__ void start() const {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            issue(0);
+            issue(1);
+        }
+    }
+    __device__ __forceinline__ void wait(int it) const {
+        const uint32_t b = bar + 8u * (uint32_t)(it & 1);
+        if (!mbar_wait(b, (phase + (unsigned)(it >> 1)) & 1u)) {
+            if (fault && (threadIdx.x & 31) == 0) atomicOr(fault, 1u);
+            mbar_wait(b, (phase + (unsigned)(it >> 1)) & 1u);  // let a late copy land before reuse
+        }
+    }
+    // every lane has read the stage of iteration it: reuse it for it + 2
+    __device__ __forceinline__ void refill(int it) const {
+        if (it + 2 >= C::kIters) return;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) issue(it + 2);
+    }
+    // the task's row in the stage (lane / R1 = row of the iteration, lane % R1 = n1)
+    __device__ __forceinline__ const float2 *task(int it, int lane) const {
+        return base + (it & 1) * C::kRows * G::N + (lane / G::R1) * G::N + lane % G::R1;
+    }
+};
+
 // shared-memory layout of the position kernel (float2 units after the field)
 template <class G>
 struct Smem {
-    // TW: twiddles [k2][n1]; TWT (right after): the same transposed, [n1][k2]
+    // TW: twiddles [k2][n1]; TWT (right after): the same transposed, [n1][k2];
+    // STG: staged saved-wave rows (16-byte aligned), BAR: their mbarriers
     static constexpr int TW = G::FIELD, TWT = TW + G::N, E1 = TWT + G::N, E2 = E1 + G::N, PY = E2 + G::N,
-                         PX = PY + G::N, END = PX + G::N;
+                         PX = PY + G::N, STG = (PX + G::N + 1) & ~1, BAR = STG + StageCfg<G>::kStageF2,
+                         END = BAR + StageCfg<G>::kBarF2;
 };
 // column pass A reads its twiddles from the transposed table two at a time
 // (R2 even): R2/2 16-byte loads per task instead of R2-1 8-byte ones
@@ -281,7 +385,7 @@ struct PositionKernel {
     }
 
     static __device__ __forceinline__ void run(const LaunchArgs &a, const TiltDev &t, int p, float2 *buf, float2 *save,
-                               double *red) {
+                               double *red, unsigned &stage_phase) {
         const float2 *tw = buf + Smem<G>::TW;
         float2 *e1 = buf + Smem<G>::E1;
         float2 *e2 = buf + Smem<G>::E2;
@@ -417,6 +521,11 @@ struct PositionKernel {
         }
 
         // ---- far field, error, residual (mset.cu:186-227) ----
+        if constexpr (StageCfg<G>::kOn) {
+            // the saved waves were written through the generic proxy; the
+            // adjoint's bulk copies read them through the async proxy
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+        }
         row_passB<G, -1>(buf);
         sync_rowcol();
         col_passA<G, -1, true, kColTw<G>>(buf, tw);
@@ -520,6 +629,7 @@ struct PositionKernel {
               for (int i = threadIdx.x; i < G::FIELD; i += G::NT) mine[i] = buf[i];
               sync_all<G>();
               recompute(a, t, s0, s1, buf, tw, py, px, save + (size_t)seg * NN, recbuf);
+              if constexpr (StageCfg<G>::kOn) asm volatile("fence.proxy.async.global;" ::: "memory");
               sync_all<G>();
               for (int i = threadIdx.x; i < G::FIELD; i += G::NT) buf[i] = mine[i];
               sync_all<G>();
@@ -532,17 +642,28 @@ struct PositionKernel {
                                      : (ws == s0 ? save + (size_t)seg * NN : recbuf + (size_t)(ws - s0 - 1) * NN);
             // the saved wave was written long ago (DRAM); have it in L2 by the row pass
             prefetch_l2(wave, (unsigned)(sizeof(float2) * NN));
-            const L1Rows<G> l1{Tslab ? reinterpret_cast<const char *>(Tslab + (size_t)s * NN) : nullptr,
-                               reinterpret_cast<const char *>(wave)};
+            constexpr bool kStg = StageCfg<G>::kOn;
+            using APre = std::conditional_t<kStg, T1Pre<G>, TSPre<G>>;
+            using L1A = std::conditional_t<kStg, L1Rows<G, false, true>, L1Rows<G>>;
+            const L1A l1{Tslab ? reinterpret_cast<const char *>(Tslab + (size_t)s * NN) : nullptr,
+                         kStg ? nullptr : reinterpret_cast<const char *>(wave)};
             l1_first<G>(l1);  // this slab's first row-pass-A iteration, two passes ahead
+            using SG = std::conditional_t<kStg, RowStage<G>, NoStage>;
+            SG stg{};
+            if constexpr (kStg) {
+                stg = RowStage<G>{buf + Smem<G>::STG + 2 * StageCfg<G>::kRows * N * Own<G>::warp(),
+                                  (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 16u * Own<G>::warp(),
+                                  wave, Own<G>::warp() * Own<G>::RPW, stage_phase, a.fault};
+                stg.start();
+            }
             col_passA<G, +1, false, kColTw<G>>(buf, tw);
             sync_rowcol();
             row_passB<G, +1>(buf);
             sync_rows();
-            // both operands are loaded before the task's shared-memory reads:
-            // loading either inside the op instead (fewer live registers at
-            // R2 = 16) exposes its latency and cost 17-22% at n = 256
-            auto pf = [&](int y, int n1, TSPre<G> &pre) {
+            // the operands are loaded before the task's shared-memory reads:
+            // loading them inside the op instead (fewer live registers at
+            // R2 = 16) exposes their latency and cost 17-22% at n = 256
+            auto pf = [&](int y, int n1, APre &pre) {
                 const float2 *sv = wave + (size_t)y * N + n1;
                 if constexpr (MODE == kBatch || MODE == kBatchCk) {
                     // the slab row's address once per task (the descriptor
@@ -551,28 +672,32 @@ struct PositionKernel {
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
                         pre.t[j] = tr[R1 * j];
-                        pre.w[j] = sv[R1 * j];
+                        if constexpr (!kStg) pre.w[j] = sv[R1 * j];
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < R2; ++j) {
                         pre.t[j] = trans(a, t, s, y, n1 + R1 * j);
-                        pre.w[j] = sv[R1 * j];
+                        if constexpr (!kStg) pre.w[j] = sv[R1 * j];
                     }
                 }
+                (void)sv;
             };
-            auto gradop = [&](int y, int n1, float2 *v, const TSPre<G> &pre) {
-                // the gradient row's address in a register: an atomic through a
+            auto gradop = [&](int y, int n1, float2 *v, const APre &pre, const float2 *wst) {
+                // the gradient row's address in a register: a store through a
                 // generic pointer could alias the descriptor in shared memory,
-                // which would otherwise be re-read after every atomic
+                // which would otherwise be re-read after every store
                 double *grow = nullptr;
                 if constexpr (MODE != kSeq && MODE != kStep) grow = gslab + (size_t)s * NN + (size_t)y * N;
 #pragma unroll
                 for (int j = 0; j < R2; ++j) {
                     const int x = n1 + R1 * j;
                     const float2 T = pre.t[j];
+                    float2 W;
+                    if constexpr (kStg) W = wst[R1 * j];
+                    else W = pre.w[j];
                     // g = i conj(T) conj(psi) chi
-                    const float2 u = cmulc(cmulc(v[j], T), pre.w[j]);
+                    const float2 u = cmulc(cmulc(v[j], T), W);
                     const float gre = -u.y;  // Re(i u)
                     if constexpr (MODE == kSeq) {
                         int z0, z1;
@@ -603,13 +728,28 @@ struct PositionKernel {
                             for (int z = z0; z < z1; ++z) V[(size_t)z * NN + (size_t)y * N + x] += du;
                         }
                     } else {
-                        atomicAdd(grow + x, (double)gre);
+                        // FP64 sum over positions: a reduction without return
+                        // value straight to the global address
+                        asm volatile("red.global.add.f64 [%0], %1;" ::"l"(__cvta_generic_to_global(grow + x)),
+                                     "d"((double)gre)
+                                     : "memory");
                     }
                     v[j] = cmulc(v[j], T);  // chi <- conj(T) chi
                 }
             };
+            auto run_rowA = [&](auto out) {
+                constexpr int OUT = decltype(out)::value;
+                if constexpr (kStg) {
+                    row_passA_pf<G, +1, OUT, APre>(buf, tw, pf, gradop, l1, stg);
+                } else {
+                    row_passA_pf<G, +1, OUT, APre>(
+                        buf, tw, pf,
+                        [&](int y, int n1, float2 *v, const APre &pre) { gradop(y, n1, v, pre, nullptr); }, l1);
+                }
+            };
+            if constexpr (kStg) stage_phase += StageCfg<G>::kIters / 2;
             if (s > 0) {
-                row_passA_pf<G, +1, -1, TSPre<G>>(buf, tw, pf, gradop, l1);
+                run_rowA(std::integral_constant<int, -1>{});
                 sync_rows();
                 row_passB<G, -1>(buf);
                 sync_rowcol();
@@ -620,7 +760,7 @@ struct PositionKernel {
                 });
                 sync_cols<G>();
             } else {
-                row_passA_pf<G, +1, 0, TSPre<G>>(buf, tw, pf, gradop, l1);
+                run_rowA(std::integral_constant<int, 0>{});
                 sync_all<G>();
             }
           }
@@ -756,6 +896,16 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     // sit in front of every dependent load
     __shared__ TiltDev s_tilt;
     load_tables<G>(buf, a);
+    if constexpr (StageCfg<G>::kOn) {
+        // two mbarriers per warp for the bulk-staged saved-wave rows (one arrival each)
+        if ((threadIdx.x & 31) == 0) {
+            const uint32_t b = (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 16u * (threadIdx.x >> 5);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b + 8u) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    unsigned stage_phase = 0;  // completed phases of each staging mbarrier
     // one set of saved-wave slots per field (per cluster when the field is split)
     float2 *save = a.save + (size_t)(blockIdx.x / G::CL) * a.slots * G::N * G::N;
     // (cluster) every CTA has started before any distributed shared-memory access
@@ -764,11 +914,11 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     if constexpr (MODE == kSeq) {
         if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
         sync_all<G>();
-        for (int p = 0; p < s_tilt.npos; ++p) K::run(a, s_tilt, p, buf, save, red);
+        for (int p = 0; p < s_tilt.npos; ++p) K::run(a, s_tilt, p, buf, save, red, stage_phase);
     } else if constexpr (MODE == kStep) {
         if (threadIdx.x == 0) s_tilt = a.tilts[a.seq_tilt];
         sync_all<G>();
-        K::run(a, s_tilt, a.step_k, buf, save, red);
+        K::run(a, s_tilt, a.step_k, buf, save, red, stage_phase);
     } else {
         int cur = -1;
         for (;;) {
@@ -793,7 +943,7 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
                 __syncthreads();
                 cur = tp.x;
             }
-            K::run(a, s_tilt, tp.y, buf, save, red);
+            K::run(a, s_tilt, tp.y, buf, save, red, stage_phase);
         }
     }
 }
@@ -1003,6 +1153,10 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
 // scrambled layouts): a choice for the autotuner, table entry kGeo<NAME_>
 #define MSET_DEFINE_GEO_VARIANT(NAME_, N_, R1_, NT_, MINB_) \
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_>))
+// the same window and thread shape with the adjoint's saved-wave rows staged
+// in shared memory by bulk copies (StageCfg)
+#define MSET_DEFINE_GEO_STAGED(NAME_, N_, R1_, NT_, MINB_) \
+    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_, true>))
 // a field split by rows over a cluster of CL_ CTAs
 #define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
 #define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_, MINB_) \
@@ -1016,6 +1170,7 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
                                        Geo##NAME_::NT,                                 \
                                        Geo##NAME_::CL,                                 \
                                        smem_bytes<Geo##NAME_>(),                       \
+                                       StageCfg<Geo##NAME_>::kOn ? 1 : 0,              \
                                        &geo_max_clusters<Geo##NAME_>,                  \
                                        &geo_positions<Geo##NAME_>,                     \
                                        &geo_prep_amp<Geo##NAME_>,                      \
