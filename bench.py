@@ -11,14 +11,23 @@ tilt, in one persistent launch.  Inputs (measured amplitudes 1.4 GB) exceed
 L2, so no flush is needed between steps.
 
 Beside the headline (rank 0, mid workload only; --no-* skips them): the full
-iteration as one CUDA graph, the sequential plain forms (this library's and
-the reference's own CUDA module), the uneven-size 6-series group pass with the
-autotuner, the 256^2-window cluster kernel on 3 tilts of the large geometry,
-and the FP64 CPU port on a sample.
+iteration as one CUDA graph, the plain form of the pass (one launch per tilt,
+one CTA per position, no graph, no checkpointing), the sequential forms with
+reference semantics (this library's mset_run and the reference's own CUDA
+module), the uneven-size 6-series group pass with the autotuner, the
+256^2-window cluster kernel on 3 tilts of the large geometry, and the
+single-precision CPU port on a sample.
 
-One JSON line on stdout (rank 0).  --impl reference times the FP64 CPU port
-of the reference's path (the reference's own CPU path is MATLAB code, which
-is not available here) on a bounded sample of the same workload.
+Under torchrun (--gpus N > 1) the 21 tilts are split over the ranks
+(mset_b200.distributed.tilt_shard): one specimen, each rank its own tilts,
+the whole workload's slice-propagations over the slowest rank's time (strong
+scaling); the iteration adds the one all-reduce of the FP64 lab-frame
+gradient per iteration.
+
+One JSON line on stdout (rank 0).  --impl reference times the reference's CPU
+path (MATLAB code in single precision, not available here) as its
+single-precision C port (oracle/cpu_fp32.c) on the host cores, on a bounded
+sample of the same workload.
 """
 from __future__ import annotations
 
@@ -37,9 +46,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 
-# DRAM bytes per slice-propagation of k_positions at n = 128, 64 slabs,
-# measured with ncu on 128 positions (8192 units): (1.077490 + 1.111658) GB
-TRAFFIC_PER_UNIT = (1.077490e9 + 1.111658e9) / 8192
+# DRAM bytes per slice-propagation of k_positions at n = 128, 64 slabs:
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
+# kernel on 2 tilts x 64 positions (8192 units): (1.076925 + 1.109599) GB.
+# A constant of this bench (ncu does not run inside it), scaled by units.
+TRAFFIC_PER_UNIT = (1.076925e9 + 1.109599e9) / 8192
 
 
 def flops_per_unit(n: int) -> float:
@@ -114,37 +125,41 @@ def measured_peaks() -> dict:
 
 
 # ---------------------------------------------------------------------------
-def build_problem(cfg_name: str, rank: int, device: int, method: int = 1, adjoint: int = 0):
+def build_problem(cfg_name: str, device: int, tilts=None, method: int = 1, adjoint: int = 0):
+    """The configuration's specimen (one seed for every rank) and a batched
+    session holding the tilts `tilts` (default: all) with Poisson counts of
+    the library's own forward model at the true volumes and the state at half
+    the true potential (a mid-reconstruction estimate)."""
     import torch
 
     from mset_b200 import synth
     from mset_b200.batch import BatchSession
 
     cfg = synth.CONFIGS[cfg_name]
-    cfg = synth.Config(**{**cfg.__dict__, "seed": cfg.seed + 7919 * rank})
     spec = synth.make_specimen(cfg)
-    npos = [spec.scan_x.size] * cfg.n_tilts
+    tilts = list(range(cfg.n_tilts)) if tilts is None else list(tilts)
+    vols = [spec.volumes[j] for j in tilts]
+    npos = [spec.scan_x.size] * len(tilts)
     bs = BatchSession(n=cfg.window, nz=cfg.vol[0], npos=npos, prop=spec.prop, sigma=spec.sigma,
                       potential_pixelsize=cfg.dx, slice_binning=cfg.slice_binning, method=method,
                       adjoint=adjoint, device=device)
     if cfg.name.startswith("large"):
         bs.set_amplitude_bf16(True)  # measured counts stored as BF16 (22 GB instead of 44 GB at 41 tilts)
     # simulate the measured intensities with the library's own forward model
-    for j, v in enumerate(spec.volumes):
+    for j, v in enumerate(vols):
         bs.set_tilt(j, probe=spec.probe, scan_x=spec.scan_x, scan_y=spec.scan_y,
                     measured=np.zeros((npos[j], cfg.window, cfg.window), np.float32), volume=v)
     inten = bs.simulate()
     g = torch.Generator(device=f"cuda:{device}")
-    g.manual_seed(cfg.seed + 1000)
+    g.manual_seed(cfg.seed + 1000 + 7919 * tilts[0])
     it = torch.from_numpy(inten).to(f"cuda:{device}")
     meas = torch.poisson(it.clamp_min(0), generator=g).cpu().numpy().astype(np.float32)
     del it, inten
-    # reconstruction state: half the true potential (a mid-iteration estimate)
     off = 0
-    for j, v in enumerate(spec.volumes):
+    for j, v in enumerate(vols):
         bs.set_tilt(j, measured=meas[off:off + npos[j]], volume=0.5 * v)
         off += npos[j]
-    return cfg, spec, bs, meas
+    return cfg, spec, bs, meas, tilts
 
 
 def workload_name(cfg, ns: int, positions: int) -> str:
@@ -165,11 +180,19 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    cfg, spec, bs, meas = build_problem(args.config, rank, local)
+    from mset_b200 import synth
+    from mset_b200.distributed import tilt_shard
+    ntilts = synth.CONFIGS[args.config].n_tilts
+    shard = tilt_shard(ntilts, world, rank)
+    if not shard:
+        raise SystemExit(f"--gpus {world} exceeds the {ntilts} tilts of the workload")
+    cfg, spec, bs, meas, shard = build_problem(args.config, local, shard)
     n = cfg.window
     ns = -(-cfg.vol[0] // cfg.slice_binning)
-    positions = int(bs.npos.sum())
+    positions = int(bs.npos.sum())            # this rank's positions
     units = positions * ns
+    positions_total = spec.scan_x.size * cfg.n_tilts
+    units_total = positions_total * ns          # the whole workload, over all ranks
 
     # warm-up (untimed)
     for _ in range(max(args.warmup, 0)):
@@ -188,14 +211,14 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    value = world * units / (ms / 1e3)
+    value = units_total / (ms / 1e3)
 
     # full batched iteration as one CUDA graph: rotate -> forward -> loss ->
     # adjoint -> rotate back -> update -> positivity -> TV-FISTA (lambda 1e-3)
     it_ms = None
     cubic = cfg.vol[0] == cfg.vol[1] == cfg.vol[2] and cfg.vol[0] <= 160
     if not args.no_iter and cubic:
-        bs.iteration_setup(cfg.vol[0], spec.angles, positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter,
+        bs.iteration_setup(cfg.vol[0], spec.angles[shard], positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter,
                            tv_fista=True)
         bs.set_rec(0.5 * spec.lab)
         k_it = max(1, min(args.steps, 3))
@@ -227,6 +250,14 @@ def run_ours(args):
     # side measurements: one GPU only (under torchrun the other ranks would
     # wait for rank 0 in the next collective)
     plain = reference_cuda(args, cfg, spec, meas, units_per_pos=ns) if (world == 1 and not args.no_plain) else None
+    if plain is not None:
+        # the plain form of the same pass on the same resident data
+        pms = bs.time_plain(max(1, min(args.steps, 3)))
+        plain["plain_batched"] = {
+            "value": units / (pms / 1e3), "unit": "slice-propagations/s", "ms_per_pass": pms,
+            "what": "the same pass in plain form: one launch per tilt with one CTA per position (no persistent "
+                    "queue across tilts, no CUDA graph, no checkpointing)"}
+        plain["batched_over_plain"] = pms / ms
     side = world == 1 and args.config == "mid"
     uneven = uneven_batch(args, local) if (side and not args.no_uneven) else None
     large = large_window(args, local) if (side and not args.no_large) else None
@@ -239,19 +270,20 @@ def run_ours(args):
         return t.numpy()
 
     vols = []
-    for v in spec.volumes:
+    for j in shard:
+        v = spec.volumes[j]
         hv = pinned(v.shape, torch.float32)
         hv[...] = 0.5 * v
         vols.append(hv)
-    grad = pinned((cfg.n_tilts, ns, n, n), torch.float64)
-    err = pinned((cfg.n_tilts,), torch.float64)
+    grad = pinned((len(shard), ns, n, n), torch.float64)
+    err = pinned((len(shard),), torch.float64)
     import ctypes as C
     from mset_b200._lib import check, dptr, fptr
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for j in range(cfg.n_tilts):
+        for j in range(len(shard)):
             check("mset_batch_set_volume", bs._lib.mset_batch_set_volume(bs._h, j, fptr(vols[j])))
         check("mset_batch_gradient", bs._lib.mset_batch_gradient(bs._h, dptr(grad), None, None, dptr(err)))
     e2e_s = (time.perf_counter() - t0) / e2e_steps
@@ -266,7 +298,7 @@ def run_ours(args):
         fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s, FMA counted as 2
         flop = units * flops_per_unit(n) + positions * flops_per_position(n)
         achieved = flop / (ms / 1e3) / 1e12
-        cpu = cpu_baseline(args, cfg, spec, meas) if (not args.no_cpu and world == 1) else None
+        cpu = cpu_baseline(args, cfg, spec) if (not args.no_cpu and world == 1) else None
         line = {
             "metric": "slice-propagations/s (fwd+adjoint)",
             "value": value,
@@ -277,24 +309,26 @@ def run_ours(args):
             "ms_per_step": ms,
             "s_per_step": ms / 1e3,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong",
             "vs_baseline": None,
             "dtype": "fp32 (complex64 propagation, fp64 reductions)",
             "data": "synthetic (seeded fcc Cu/Au-like Gaussian-atom lattice, Poisson 1e4 e-/probe)",
-            "config": {"workload": workload_name(cfg, ns, positions),
-                       "positions_per_gpu": positions, "slabs": ns, "window": n,
-                       "units_per_step_per_gpu": units, "persistent_ctas": bs.shape()["grid"],
-                       "l2": f"inputs larger than L2 ({meas_bytes / 1e9:.1f} GB measured patterns)",
-                       "parallelism": f"tilt replicas x{world}"},
+            "config": {"workload": workload_name(cfg, ns, positions_total),
+                       "positions": positions_total, "positions_rank0": positions, "slabs": ns, "window": n,
+                       "units_per_step": units_total, "persistent_ctas": bs.shape()["grid"],
+                       "l2": f"inputs larger than L2 ({meas_bytes / 1e9:.1f} GB measured patterns per GPU)",
+                       "parallelism": f"tilts sharded over {world} GPU(s): rank 0 holds tilts "
+                                      f"{shard[0]}-{shard[-1]} of {cfg.n_tilts}"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak,
-                         # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_positions launch on
-                         # the mid_s capture (128 positions: 1.0775 GB + 1.1117 GB), scaled by units
-                         # (n^2 scaling to other windows: both terms are per-pixel)
+                         # DRAM bytes of one launch: the per-unit figure of an ncu capture of the same
+                         # kernel (TRAFFIC_PER_UNIT), scaled by units (n^2 for other windows: both terms
+                         # are per-pixel); a constant of this bench, not measured per run
                          "traffic": TRAFFIC_PER_UNIT * units * (n / 128.0) ** 2,
-                         "traffic_note": "bytes per launch from the ncu capture of the same kernel on 128 positions "
-                                         "(profiles/k_positions_mid_s.md), scaled by slice-propagations; "
-                                         "algorithmic bytes per unit 16*n^2 (saved wave write + read) + "
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_positions on "
+                                           "2 tilts x 64 positions of this geometry, per slice-propagation, "
+                                           "times the launch's slice-propagations (constant, not per run)",
+                         "traffic_note": "algorithmic bytes per unit 16*n^2 (saved wave write + read) + "
                                          "4*n^2/slabs (amplitudes)",
                          "algorithmic_bytes": units * (16 * n * n + 4 * n * n / ns),
                          "peak_source": f"nominal FP32 CUDA-core peak 148 SM x 128 lanes x 2 x {sm_max:.0f} MHz "
@@ -310,15 +344,17 @@ def run_ours(args):
                              "traffic": TRAFFIC_PER_UNIT * units * (n / 128.0) ** 2,
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
                              else "fallback 6.65 TB/s"},
-            "e2e": {"value": world * units / e2e_s, "unit": "slice-propagations/s", "host_memory": "pinned",
+            "e2e": {"value": units_total / e2e_s, "unit": "slice-propagations/s", "host_memory": "pinned",
                     "h2d_bytes_per_step": int(sum(v.nbytes for v in vols)),
                     "d2h_bytes_per_step": int(grad.nbytes + err.nbytes)},
             "iteration": None if it_ms is None else {
                 "s_per_iteration": it_ms / 1e3,
-                "what": "one CUDA-graph replay: 21 inverse Fourier-shear rotations, transmission slabs, the "
-                        "batched forward+adjoint pass, 21 forward rotations of the gradient, update, positivity, "
-                        f"TV-FISTA lambda 1e-3 x {args.tv_iter} iterations, probe and position updates",
-                "slice_propagations_per_s": world * units / (it_ms / 1e3)},
+                "what": f"{cfg.n_tilts} inverse Fourier-shear rotations, transmission slabs, the batched "
+                        f"forward+adjoint pass, {cfg.n_tilts} forward rotations of the gradient, update, positivity, "
+                        f"TV-FISTA lambda 1e-3 x {args.tv_iter} iterations, probe and position updates; one CUDA "
+                        "graph" + ("" if world == 1 else f" per phase on each of {world} GPUs with the tilts sharded "
+                                   "and one NCCL all-reduce of the FP64 lab-frame gradient between the phases"),
+                "slice_propagations_per_s": units_total / (it_ms / 1e3)},
             "plain_forms": plain,
             "uneven_batch": uneven,
             "large_window": large,
@@ -335,40 +371,50 @@ def run_ours(args):
 
 def reference_cuda(args, cfg, spec, meas, units_per_pos: int) -> dict:
     """Sequential (reference-semantics) GPU forms on the first positions of
-    tilt 0: this library's plain fused kernel (mset_run, one CTA walking the
-    positions in order) and, when built, the reference's own CUDA module
-    (src/CUDA/mset.cu + cuFFT via oracle/_ref).  Both: CUDA-event free host
-    timing around a synchronous call, after one warm-up call."""
+    tilt 0: this library's mset_run (positions in order, each updating
+    volume, probe and position; each position's field split over an 8-CTA
+    cluster, and on one CTA) and, when built, the reference's own CUDA module
+    (src/CUDA/mset.cu + cuFFT via oracle/_ref).  Host time around the
+    synchronous call, median of 3 repeats after one warm-up, the upload
+    outside the timed call."""
     from mset_b200 import Session
 
     k = args.plain_positions
-    n = cfg.window
     v = 0.5 * spec.volumes[0]
     sx, sy, me = spec.scan_x[:k], spec.scan_y[:k], meas[:k]
     step = (1e-3, 1e-6, 1e-3)
+    units = k * units_per_pos
     out = {"positions": k, "slabs": units_per_pos,
            "what": "run_mset over the first positions of tilt 0 (sequential per-position updates)"}
-    with Session() as s:
-        for rep in range(2):
-            s.upload(v, spec.probe, spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx, scan_x=sx, scan_y=sy,
-                     measured=me, step_size=step, slice_binning=cfg.slice_binning)
+
+    def timed(run, upload, reps=4):
+        ts = []
+        for _ in range(reps):
+            upload()
             t0 = time.perf_counter()
-            s.run(1)
-            dt = time.perf_counter() - t0
-        out["plain_gpu"] = {"value": k * units_per_pos / dt, "unit": "slice-propagations/s", "seconds": dt}
+            run()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts[1:]))
+
+    for split, key in ((True, "plain_gpu"), (False, "plain_gpu_one_cta")):
+        with Session() as s:
+            s.set_sequential_split(split)
+            up = lambda: s.upload(v, spec.probe, spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx, scan_x=sx,
+                                  scan_y=sy, measured=me, step_size=step, slice_binning=cfg.slice_binning)
+            dt = timed(lambda: s.run(1), up)
+            out[key] = {"value": units / dt, "unit": "slice-propagations/s", "seconds": dt,
+                        "ctas_per_position": s.sequential_split()}
     try:
         from oracle import refharness
         if refharness.available():
-            for rep in range(2):
-                r = refharness.RefSession()
-                r.upload(v, spec.probe, spec.prop, sigma=spec.sigma, dz=cfg.dx, scan_x=sx, scan_y=sy, measured=me,
-                         step=step, binning=cfg.slice_binning)
-                t0 = time.perf_counter()
-                r.run(1)
-                dt = time.perf_counter() - t0
-            out["reference_cuda"] = {"value": k * units_per_pos / dt, "unit": "slice-propagations/s", "seconds": dt,
+            r = refharness.RefSession()
+            up = lambda: r.upload(v, spec.probe, spec.prop, sigma=spec.sigma, dz=cfg.dx, scan_x=sx, scan_y=sy,
+                                  measured=me, step=step, binning=cfg.slice_binning)
+            dt = timed(lambda: r.run(1), up)
+            out["reference_cuda"] = {"value": units / dt, "unit": "slice-propagations/s", "seconds": dt,
                                      "what": "the reference's src/CUDA module (cuFFT, ~18*slabs+60 launches per "
                                              "position), compiled unchanged for sm_100a"}
+            out["plain_gpu_over_reference_cuda"] = out["reference_cuda"]["seconds"] / out["plain_gpu"]["seconds"]
     except Exception as e:  # the checker build is optional
         out["reference_cuda"] = {"unavailable": str(e)[:200]}
     return out
@@ -443,7 +489,7 @@ def large_window(args, device: int) -> dict:
     the batched gradient pass, device-timed."""
     import torch
 
-    cfg, spec, bs, meas = build_problem("large_s", 0, device)
+    cfg, spec, bs, meas, _ = build_problem("large_s", device)
     del meas
     ns = -(-cfg.vol[0] // cfg.slice_binning)
     units = int(bs.npos.sum()) * ns
@@ -507,63 +553,75 @@ def large_iteration(args, device: int) -> dict:
             "workload": workload_name(cfg, ns, int(sum(npos)))}
 
 
-def cpu_sample_positions(cores: int) -> int:
-    return int(max(8, min(96, 6 * cores)))
+def host_sample(cfg_name: str, k: int):
+    """A bounded sample of the workload for the host-side baselines: k
+    positions spread over the scan of the specimen's 0-degree tilt (same
+    window, volume, slabs and scan as the workload), their intensities from the
+    single-precision forward model (oracle/cpu_fp32.c) at the true volume with
+    seeded Poisson counts, and the state at half the true potential.  Built on
+    the host alone, so the reference arm (which uses no GPU) and the CPU
+    baseline of this arm time the same bytes."""
+    import dataclasses
+
+    from mset_b200 import synth
+    from oracle import oracle as O
+
+    cfg = synth.CONFIGS[cfg_name]
+    spec = synth.make_specimen(dataclasses.replace(cfg, n_tilts=1))
+    idx = np.linspace(0, spec.scan_x.size - 1, min(k, spec.scan_x.size)).round().astype(int)
+    sx, sy = spec.scan_x[idx], spec.scan_y[idx]
+    vt = spec.volumes[0]
+    inten = O.simulate_fp32(vt, spec.probe, spec.prop, sx, sy, sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning)
+    meas = synth.poisson(inten, cfg.seed + 1000)
+    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    return dict(cfg=cfg, spec=spec, V=(0.5 * vt).astype(np.float32), sx=sx, sy=sy, meas=meas, ns=ns)
 
 
-def cpu_baseline(args, cfg, spec, meas) -> dict:
-    """FP64 CPU port (oracle) on a bounded sample of the same workload."""
+def host_pass(smp: dict, cores: int):
+    from oracle import oracle as O
+    c = smp["cfg"]
+    return O.batched_tilt_fp32(smp["V"], smp["spec"].probe, smp["spec"].prop, smp["sx"], smp["sy"], smp["meas"],
+                               sigma=smp["spec"].sigma, dz=c.dx, binning=c.slice_binning, nthreads=cores)
+
+
+def cpu_baseline(args, cfg, spec) -> dict:
+    """The single-precision CPU port of the reference's path (oracle/cpu_fp32.c,
+    OpenMP over positions, all host threads) on a bounded sample of the same
+    workload (about 10 s of host work on a 16-thread host)."""
     from oracle import oracle as O
 
     cores = O.max_threads()
-    k = cpu_sample_positions(cores)
-    ns = -(-cfg.vol[0] // cfg.slice_binning)
+    smp = host_sample(args.config, min(1024, 32 * cores))
+    k, ns = smp["sx"].size, smp["ns"]
     t0 = time.perf_counter()
-    O.batched_tilt(0.5 * spec.volumes[0], spec.probe, spec.prop, spec.scan_x[:k], spec.scan_y[:k], meas[:k],
-                   sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+    host_pass(smp, cores)
     dt = time.perf_counter() - t0
-    # the reference's sequential semantics (per-position updates) on one core
-    ks = 4
-    t1 = time.perf_counter()
-    O.run_tilt(0.5 * spec.volumes[0], spec.probe, spec.prop, spec.scan_x[:ks], spec.scan_y[:ks], meas[:ks],
-               sigma=spec.sigma, dz=cfg.dx, step=(1e-3, 1e-6, 1e-3), binning=cfg.slice_binning)
-    dt1 = time.perf_counter() - t1
     return {"value": k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
-            "sample": f"{k} positions of tilt 0 of the same workload (FP64 C port of the reference path, "
-                      f"OpenMP over positions), {dt:.1f} s",
-            "sequential_1core": {"value": ks * ns / dt1, "unit": "slice-propagations/s", "cores": 1,
-                                 "sample": f"run_mset semantics (per-position updates) over {ks} positions of "
-                                           f"tilt 0, FP64 C port, {dt1:.1f} s"}}
+            "dtype": "fp32",
+            "sample": f"{k} positions of the 0-degree tilt of the same geometry ({ns} slabs each), single-precision C port "
+                      f"of the reference's CPU path (its MATLAB STEP02/STEP03 run in single), {dt:.1f} s"}
 
 
 def run_reference(args):
-    """The reference arm: the FP64 CPU port of the reference's path on the
+    """The reference arm: the reference's CPU path (MATLAB STEP02/STEP03 in
+    single precision, unavailable here) as its single-precision C port on the
     host cores, on a bounded sample of the same workload per step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from mset_b200 import synth
     from oracle import oracle as O
 
-    cfg = synth.CONFIGS[args.config]
-    spec = synth.make_specimen(cfg, with_volumes=False)
-    rng = np.random.default_rng(cfg.seed)
-    pos, peak = synth.atoms(cfg, rng)
-    v = synth.pad_lateral(synth.voxelise(pos, peak, cfg.vol, cfg.dx, cfg.blob_sigma), cfg.window).astype(np.float32)
     cores = O.max_threads()
-    k = max(4, cpu_sample_positions(cores) // 4)
-    n = cfg.window
-    meas = np.full((k, n, n), 1.0, np.float32)
-    ns = -(-cfg.vol[0] // cfg.slice_binning)
-    for _ in range(max(args.warmup, 0) and 1):
-        O.batched_tilt(0.5 * v, spec.probe, spec.prop, spec.scan_x[:1], spec.scan_y[:1], meas[:1],
-                       sigma=spec.sigma, dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+    smp = host_sample(args.config, max(32, 8 * cores))
+    cfg, k, ns = smp["cfg"], smp["sx"].size, smp["ns"]
+    for _ in range(max(args.warmup, 0)):
+        host_pass(smp, cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.batched_tilt(0.5 * v, spec.probe, spec.prop, spec.scan_x[:k], spec.scan_y[:k], meas, sigma=spec.sigma,
-                       dz=cfg.dx, binning=cfg.slice_binning, nthreads=cores)
+        host_pass(smp, cores)
     dt = (time.perf_counter() - t0) / args.steps
     value = k * ns / dt
+    nz, ny, nx = cfg.vol
     line = {
         "impl": "reference",
         "metric": "slice-propagations/s (fwd+adjoint)",
@@ -574,15 +632,17 @@ def run_reference(args):
         "warmup": args.warmup,
         "ms_per_step": dt * 1e3,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong",
         "vs_baseline": None,
-        "dtype": "fp64",
+        "dtype": "fp32",
         "data": "synthetic",
-        "config": {"workload": "mid: 128^3 volume, 128^2 window, 32x32 scan, 21 tilts, 64 slabs x 2 voxels "
-                               f"(sampled: {k} positions per step)"},
+        "config": {"workload": f"{cfg.name}: {nx}x{ny}x{nz} volume, {cfg.window}^2 window, "
+                               f"{cfg.scan[0]}x{cfg.scan[1]} scan, {cfg.n_tilts} tilts, {ns} slabs x "
+                               f"{cfg.slice_binning} voxels (sampled: {k} positions of the 0-degree tilt per step)"},
         "cpu_baseline": {"value": value, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
-                         "sample": f"{k} positions x {ns} slabs per step; the reference's own CPU path is MATLAB "
-                                   "code (STEP02/STEP03), unavailable on this box, so its FP64 C port is timed"},
+                         "sample": f"{k} positions x {ns} slabs per step; the reference's CPU path is MATLAB "
+                                   "code (STEP02/STEP03) in single precision, unavailable on this box, so its "
+                                   "single-precision C port (oracle/cpu_fp32.c) is timed"},
         "e2e": {"value": value, "unit": "slice-propagations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

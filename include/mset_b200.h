@@ -151,6 +151,16 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
  * instead of per position).  rvol_out float [nz][n][n], probe_out float
  * [n][n][2]; either may be NULL. */
 int mset_read_state(mset_session *s, float *rvol_out, float *probe_out);
+/* The sequential pass (mset_run) and the per-position steps walk one position
+ * at a time, so one position's field is all the parallel work there is.
+ * Where a cluster geometry is compiled for the window (n = 128: 8 CTAs of 16
+ * rows), that field is split over a thread-block cluster (distributed shared
+ * memory) and each position runs on several SMs; results are those of the
+ * one-CTA kernel up to the order of the cluster's partial sums.
+ * mset_set_sequential_split(s, 0) keeps one CTA per field; on by default.
+ * mset_sequential_split returns the CTAs per field the sequential modes use. */
+int mset_set_sequential_split(mset_session *s, int on);
+int mset_sequential_split(mset_session *s);
 
 /* global-session shims with the MEX's lifetime (one implicit session per
  * process, recreated by every upload, mex_main.cu:13, 56) */
@@ -210,6 +220,11 @@ int mset_batch_get_tilt(mset_session *s, int j, float *volume, float *probe, flo
  * `reps` times on resident data and return the mean device time per pass in
  * milliseconds measured with CUDA events on the session stream */
 int mset_batch_time(mset_session *s, int reps, double *ms_per_pass);
+/* the plain form of the same pass, device-timed over reps: one launch per
+ * tilt with one CTA per position (no persistent queue across tilts, no CUDA
+ * graph, no checkpointing; saved waves for every position of the largest
+ * tilt), the same kernel and results; the comparator of the batched form */
+int mset_batch_time_plain(mset_session *s, int reps, double *ms_per_pass);
 /* number of kernel launches issued by one mset_batch_gradient call */
 int mset_batch_launch_count(mset_session *s);
 

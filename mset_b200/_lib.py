@@ -45,6 +45,9 @@ SIGNATURES = {
     "mset_forward_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, _F, _F, _F, _F, _F]),
     "mset_adjoint_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F, C.c_int, _F, _F, _F]),
     "mset_read_state": (C.c_int, [C.c_void_p, _F, _F]),
+    "mset_set_sequential_split": (C.c_int, [C.c_void_p, C.c_int]),
+    "mset_sequential_split": (C.c_int, [C.c_void_p]),
+    "mset_batch_time_plain": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "mset_mex_upload": (C.c_int, [C.c_void_p]),
     "mset_mex_run": (C.c_int, [C.c_int, _F, _F, _F, _F, _F]),
     "mset_mex_error": (C.c_int, [C.c_int, _F]),

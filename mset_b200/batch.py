@@ -133,6 +133,13 @@ class BatchSession:
         check("mset_batch_time", self._lib.mset_batch_time(self._h, int(reps), dptr(ms)))
         return float(ms[0])
 
+    def time_plain(self, reps: int) -> float:
+        """device ms per pass of the plain form (one launch per tilt, one CTA
+        per position, no graph, no checkpointing)"""
+        ms = np.zeros(1)
+        check("mset_batch_time_plain", self._lib.mset_batch_time_plain(self._h, int(reps), dptr(ms)))
+        return float(ms[0])
+
     def set_amplitude_bf16(self, on: bool = True):
         """keep measured counts as BF16 (set before the measured patterns)"""
         check("mset_batch_set_amplitude_bf16", self._lib.mset_batch_set_amplitude_bf16(self._h, int(bool(on))))

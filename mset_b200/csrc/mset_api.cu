@@ -106,6 +106,11 @@ struct mset_session {
     float sigma = 0, dz = 0, step[3] = {0, 0, 0};
     int nsx = 0, nsy = 0;
     Plan plan{};
+    // sequential modes (kSeq, kStep): one field split over a thread-block
+    // cluster, where such a geometry is compiled for n (seq_split: in use)
+    Plan seq_plan{};
+    bool has_seq = false;
+    bool seq_split = true;
     bool ready = false;
     bool batch = false;
     // tilts (1 for the MEX-style session)
@@ -194,6 +199,7 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
     if (b > nz) b = nz;  // STEP00_INIT.m:126-128
     if (pl.cl > 1) pl.max_clusters = pl.ops->max_clusters();
     s->plan = pl;
+    s->has_seq = plan_seq_for(n, &s->seq_plan);
     s->n = n;
     s->nz = nz;
     s->b = b;
@@ -373,6 +379,10 @@ LaunchArgs base_args(mset_session *s) {
 // The position kernel waits, with a bound, for the bulk copies that stage
 // its operands in shared memory; a wait that gave up sets the session's
 // fault word.  Read (and clear) it where a call hands results back.
+// the plan of the sequential modes: the cluster geometry when compiled and
+// enabled, else the session's own
+const Plan &seq_plan(const mset_session *s) { return (s->has_seq && s->seq_split) ? s->seq_plan : s->plan; }
+
 int take_fault(mset_session *s) {
     if (!s->fault.p) return 0;
     unsigned f = 0;
@@ -542,8 +552,8 @@ int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *
     rc = refresh_tilt_table(s);
     if (rc) return rc;
     LaunchArgs a = base_args(s);
-    CKL(launch_positions(s->plan, mode, adjoint, kSeq, a, std::max(1, s->plan.cl), s->st),
-        "sequential position kernel launch");
+    const Plan &sp = seq_plan(s);
+    CKL(launch_positions(sp, mode, adjoint, kSeq, a, std::max(1, sp.cl), s->st), "sequential position kernel launch");
     TiltBufs &t = s->tilts[0];
     const size_t n2 = (size_t)s->n * s->n;
     CKL(launch_q_to_probe(s->plan, t.Q.p, s->tmpc.p, s->twn.p, s->st), "q_to_probe");
@@ -628,7 +638,8 @@ int mset_forward_position(mset_session *s, int mode, int k, float row, float col
     a.step_resi = s->step_resi.p;
     a.step_calc = s->step_calc.p;
     a.step_err = s->step_err.p;
-    CKL(launch_positions(s->plan, mode, kREF, kStep, a, std::max(1, s->plan.cl), s->st), "STEP02 launch");
+    const Plan &sp = seq_plan(s);
+    CKL(launch_positions(sp, mode, kREF, kStep, a, std::max(1, sp.cl), s->st), "STEP02 launch");
     // the waves of field 0: slot 0 = psi0, slot s + 1 = wave after slab s
     std::vector<float2> resi(resi_out ? n2 : 0);
     if (resi_out)
@@ -697,7 +708,8 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
     a.step_resi = s->step_resi.p;
     a.step_grad = s->step_grad.p;
     a.step_pos = s->step_pos.p;
-    CKL(launch_positions(s->plan, mode, adjoint, kStep, a, std::max(1, s->plan.cl), s->st), "STEP03 launch");
+    const Plan &sp = seq_plan(s);
+    CKL(launch_positions(sp, mode, adjoint, kStep, a, std::max(1, sp.cl), s->st), "STEP03 launch");
     TiltBufs &t = s->tilts[0];
     std::vector<float2> g(grad_out ? n2 * ns : 0);
     if (grad_out)
@@ -719,6 +731,17 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
     }
     s->step_k = -1;
     return take_fault(s);
+}
+
+int mset_set_sequential_split(mset_session *s, int on) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    s->seq_split = on != 0;
+    return 0;
+}
+
+int mset_sequential_split(mset_session *s) {
+    if (!s) return fail(MSET_E_ARG, "null session");
+    return (s->has_seq && s->seq_split) ? seq_plan(s).cl : 1;
 }
 
 int mset_read_state(mset_session *s, float *rvol_out, float *probe_out) {
@@ -887,6 +910,59 @@ static int batch_pass(mset_session *s) {
     rc = batch_transmission(s);
     if (rc) return rc;
     return launch_queue(s, s->method, s->adjoint, kBatch);
+}
+
+// The plain form of the pass: one launch per tilt with one CTA per position
+// (no persistent work queue across tilts, no CUDA graph), every slab's wave
+// kept (no checkpointing); the same kernel and arithmetic as batch_pass.
+static int plain_pass(mset_session *s) {
+    int rc = batch_zero(s);
+    if (rc) return rc;
+    if (s->total_pos == 0) return 0;
+    rc = batch_transmission(s);
+    if (rc) return rc;
+    const int cl = std::max(1, s->plan.cl);
+    for (size_t j = 0; j < s->tilts.size(); ++j) {
+        const int np = s->tilts[j].npos;
+        if (np == 0) continue;
+        CK(cudaMemsetAsync(s->counter.p, 0, sizeof(unsigned), s->st));
+        LaunchArgs a = base_args(s);
+        a.items = s->items.p + s->pos_off[j];
+        a.nitems = np;
+        a.ckpt = 0;
+        a.slots = save_slots(s->ns, 0);
+        CKL(launch_positions(s->plan, s->method, s->adjoint, kBatch, a, np * cl, s->st), "plain position launch");
+    }
+    return 0;
+}
+
+int mset_batch_time_plain(mset_session *s, int reps, double *ms_per_pass) {
+    Range range_("mset_batch_time_plain");
+    int rc = batch_ok(s);
+    if (rc) return rc;
+    if (reps <= 0 || !ms_per_pass) return fail(MSET_E_ARG, "bad arguments");
+    int maxp = 0;
+    for (const TiltBufs &t : s->tilts) maxp = std::max(maxp, t.npos);
+    // saved waves for one field per position of the largest tilt, all slabs
+    const int ck = s->ckpt;
+    s->ckpt = 0;
+    rc = queue_prepare(s, kBatch, std::max(1, maxp) * std::max(1, s->plan.cl));
+    if (!rc) rc = plain_pass(s);  // warm-up
+    if (rc) {
+        s->ckpt = ck;
+        return rc;
+    }
+    cudaError_t e = cudaEventRecord(s->ev0, s->st);
+    for (int r = 0; r < reps && e == cudaSuccess && !rc; ++r) rc = plain_pass(s);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev1, s->st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(s->ev1);
+    s->ckpt = ck;
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "timing the plain pass");
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *ms_per_pass = ms / reps;
+    return take_fault(s);
 }
 
 int mset_batch_gradient(mset_session *s, double *grad_out, double *probe_out, double *posdir_out, double *err_out) {

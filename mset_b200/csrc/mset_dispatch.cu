@@ -19,6 +19,36 @@ static const GeoOps *const kAllGeos[] = {
 #undef X
 };
 
+// the reference-semantics pass and the per-position steps walk one position
+// at a time through one field; these geometries split that field over a
+// thread-block cluster so one position uses several SMs
+#define MSET_SEQ_GEOS(X) X(128c8)
+#define X(N_) extern const GeoOps kSeqGeo##N_;
+MSET_SEQ_GEOS(X)
+#undef X
+static const GeoOps *const kSeqGeos[] = {
+#define X(N_) &kSeqGeo##N_,
+    MSET_SEQ_GEOS(X)
+#undef X
+};
+
+bool plan_seq_for(int n, Plan *p) {
+    for (const GeoOps *g : kSeqGeos)
+        if (g->n == n) {
+            p->n = g->n;
+            p->r1 = g->r1;
+            p->nt = g->nt;
+            p->cl = g->cl;
+            p->staged = 0;
+            p->max_clusters = 0;
+            p->smem = g->smem;
+            p->ctas_per_sm = 0;
+            p->ops = g;
+            return true;
+        }
+    return false;
+}
+
 static const GeoOps *find_geo(int n, int variant) {
     for (const GeoOps *g : kAllGeos)
         if (g->n == n && variant-- == 0) return g;

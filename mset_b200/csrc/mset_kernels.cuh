@@ -100,6 +100,9 @@ struct Plan {
 };
 // geometry `variant` (0: default) of window size n; plan_variants(n) of them exist
 bool plan_for(int n, Plan *p, int variant = 0);
+// the cluster geometry of window n for the sequential modes (kSeq, kStep),
+// when one is compiled; its scrambled layouts are plan_for(n)'s
+bool plan_seq_for(int n, Plan *p);
 int plan_variants(int n);
 int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,
                      cudaStream_t st);

@@ -1120,6 +1120,22 @@ int geo_positions(int method, int adjoint, int mode, const LaunchArgs &a, int gr
     return (int)cudaErrorInvalidValue;
 }
 
+// (a geometry whose batched queue is never launched: one cluster per call)
+inline int geo_no_clusters() { return 0; }
+
+// the modes that walk one position at a time through one field: the
+// reference-semantics pass (kSeq) and the per-position steps (kStep); a
+// geometry compiled for these alone splits that one field over a cluster
+template <class G>
+int geo_positions_seq(int method, int adjoint, int mode, const LaunchArgs &a, int grid, cudaStream_t st) {
+#define MSET_L(M, A, MO) \
+    if (method == M && adjoint == A && mode == MO) return launch_one<G, M, A, MO>(a, grid, st);
+    MSET_L(kMSET, kREF, kSeq) MSET_L(kMSET, kEXACT, kSeq) MSET_L(kSSET, kREF, kSeq) MSET_L(kSSET, kEXACT, kSeq)
+    MSET_L(kMSET, kREF, kStep) MSET_L(kMSET, kEXACT, kStep) MSET_L(kSSET, kREF, kStep) MSET_L(kSSET, kEXACT, kStep)
+#undef MSET_L
+    return (int)cudaErrorInvalidValue;
+}
+
 template <class G>
 int geo_prep_amp(const float *meas, float *amp, long npos, cudaStream_t st) {
     k_prep_amp<G><<<1184, 256, 0, st>>>(meas, amp, npos);
@@ -1157,6 +1173,24 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
 // in shared memory by bulk copies (StageCfg)
 #define MSET_DEFINE_GEO_STAGED(NAME_, N_, R1_, NT_, MINB_) \
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (Geo<N_, R1_, NT_, MINB_, true>))
+// the sequential modes only (geo_positions_seq), with one field split by rows
+// over a cluster of CL_ CTAs: table entry kSeqGeo<NAME_>
+#define MSET_DEFINE_SEQ_GEO_CL(NAME_, N_, R1_, NT_, CL_)                                \
+    namespace mset {                                                                   \
+    using SeqGeo##NAME_ = GeoCl<N_, R1_, NT_, CL_>;                                    \
+    extern const GeoOps kSeqGeo##NAME_ = {N_,                                          \
+                                          R1_,                                         \
+                                          SeqGeo##NAME_::NT,                           \
+                                          SeqGeo##NAME_::CL,                           \
+                                          smem_bytes<SeqGeo##NAME_>(),                 \
+                                          0,                                           \
+                                          &geo_no_clusters,                            \
+                                          &geo_positions_seq<SeqGeo##NAME_>,           \
+                                          &geo_prep_amp<SeqGeo##NAME_>,                \
+                                          &geo_prep_amp_bf16<SeqGeo##NAME_>,           \
+                                          &geo_prep_prop<SeqGeo##NAME_>,               \
+                                          &geo_probe_q<SeqGeo##NAME_>};                \
+    }
 // a field split by rows over a cluster of CL_ CTAs
 #define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
 #define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_, MINB_) \

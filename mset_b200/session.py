@@ -187,6 +187,18 @@ class Session:
         cplx = lambda a: None if a is None else a.view(np.complex64)[..., 0]
         return dict(grad=cplx(grad), probe=cplx(probe), row=float(rc[0]), col=float(rc[1]))
 
+    def set_sequential_split(self, on: bool) -> None:
+        """split one position's field over a thread-block cluster in run() and
+        the per-position steps (default on where compiled, n = 128)"""
+        check("mset_set_sequential_split", self._lib.mset_set_sequential_split(self._h, int(bool(on))))
+
+    def sequential_split(self) -> int:
+        """CTAs per field of the sequential modes after upload (1: one CTA)"""
+        r = self._lib.mset_sequential_split(self._h)
+        if r < 0:
+            check("mset_sequential_split", r)
+        return int(r)
+
     def read_state(self):
         """(rvol [nz][n][n] float32, probe [n][n] complex64): the session's
         volume and probe as the per-position steps left them on the device"""

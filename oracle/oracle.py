@@ -146,6 +146,49 @@ def max_threads() -> int:
     return lib().orc_max_threads()
 
 
+_lib32 = None
+
+
+def lib32() -> C.CDLL:
+    """oracle/libcpu_fp32.so: the single-precision CPU port (cpu_fp32.c)"""
+    global _lib32
+    if _lib32 is None:
+        p = os.path.join(HERE, "libcpu_fp32.so")
+        if not os.path.exists(p) or os.path.getmtime(p) < os.path.getmtime(os.path.join(HERE, "cpu_fp32.c")):
+            subprocess.run(["make", "-C", HERE, "libcpu_fp32.so"], check=True, capture_output=True)
+        L = C.CDLL(p)
+        L.cpu32_batched_tilt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _F, _F, _F,
+                                         _F, _F, _F, _D, _D, _D, _D, C.c_int]
+        L.cpu32_simulate.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _F, _F, _F, _F,
+                                     _F, _F, C.c_int]
+        _lib32 = L
+    return _lib32
+
+
+def batched_tilt_fp32(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz, binning=1, nthreads=0):
+    """The batched pass over one tilt in single precision (cpu_fp32.c; window
+    a power of two, reference adjoint formula): the same outputs as
+    batched_tilt."""
+    rv = np.ascontiguousarray(rvol, dtype=np.float32)
+    nz, n, _ = rv.shape
+    ns = -(-nz // binning)
+    pr = np.ascontiguousarray(probe, dtype=np.complex64)
+    pp = np.ascontiguousarray(prop, dtype=np.complex64)
+    sx = np.ascontiguousarray(scan_x, dtype=np.float32)
+    sy = np.ascontiguousarray(scan_y, dtype=np.float32)
+    me = np.ascontiguousarray(measured, dtype=np.float32)
+    g = np.zeros((ns, n, n))
+    pa = np.zeros((n, n, 2))
+    pd = np.zeros((sx.size, 2))
+    err = np.zeros(1)
+    rc = lib32().cpu32_batched_tilt(n, nz, binning, sigma, dz, sx.size, _f(rv),
+                                    pr.view(np.float32).ctypes.data_as(_F), pp.view(np.float32).ctypes.data_as(_F),
+                                    _f(sx), _f(sy), _f(me), _d(g), _d(pa), _d(pd), _d(err), int(nthreads))
+    if rc != 0:
+        raise ValueError("cpu_fp32: the window must be a power of two")
+    return g, pa[..., 0] + 1j * pa[..., 1], pd, float(err[0])
+
+
 def _rot_setup():
     L = lib()
     L.orc_rot3d.argtypes = [_D, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int]
@@ -185,3 +228,20 @@ def rotation_plan(M, step=11.0):
     out = np.zeros(11)
     L.orc_rotation_plan(_d(M), float(step), _d(out))
     return dict(num_step=int(out[0]), forward=bool(out[1]), mI=int(out[2]), coeffs=out[3:].copy())
+
+
+def simulate_fp32(rvol, probe, prop, scan_x, scan_y, *, sigma, dz, binning=1, nthreads=0):
+    """|Psi|^2 in the centred layout [P][n][n] of every position (single
+    precision, cpu_fp32.c): the forward model for host-side test data."""
+    rv = np.ascontiguousarray(rvol, dtype=np.float32)
+    nz, n, _ = rv.shape
+    pr = np.ascontiguousarray(probe, dtype=np.complex64)
+    pp = np.ascontiguousarray(prop, dtype=np.complex64)
+    sx = np.ascontiguousarray(scan_x, dtype=np.float32)
+    sy = np.ascontiguousarray(scan_y, dtype=np.float32)
+    out = np.zeros((sx.size, n, n), np.float32)
+    rc = lib32().cpu32_simulate(n, nz, binning, sigma, dz, sx.size, _f(rv), pr.view(np.float32).ctypes.data_as(_F),
+                                pp.view(np.float32).ctypes.data_as(_F), _f(sx), _f(sy), _f(out), int(nthreads))
+    if rc != 0:
+        raise ValueError("cpu_fp32: the window must be a power of two")
+    return out

@@ -1,7 +1,9 @@
 """Tilt sharding of the batched iteration (mset_b200/distributed.py) with
 world size 2 on CPU (gloo): two ranks each run phase 1 on half of the tilts
-with the FP64 oracle, all-reduce the lab-frame gradient, run phase 2, and end
-with the same volume, probes and positions as one process over all tilts."""
+with the FP64 oracle, all-reduce the lab-frame gradient, run phase 2 (update,
+positivity and TV-FISTA of rec / max(rec), rescaled, as the device
+iteration's phase 2), and end with the same volume, probes and positions as
+one process over all tilts."""
 import os
 
 import numpy as np
@@ -59,8 +61,13 @@ class OracleBackend:
         return contextlib.nullcontext()
 
     def phase2(self):
+        from oracle import tv
         s = self.step
         self.rec = np.maximum(self.rec + s[0] * self.g.numpy().reshape(self.rec.shape), 0)
+        if TV_LAMBDA > 0:
+            m = self.rec.max()  # Run_MSET_recon.m:267-270
+            out, _ = tv.tv_method(self.rec / m, TV_LAMBDA, TV_ITER, fista=True)
+            self.rec = m * out
         for j in self.ids:
             t = self.tilts[j]
             t["probe"] = (t["probe"] - s[1] * self._pa[j]).astype(np.complex64)
@@ -75,6 +82,7 @@ def _problem():
 
 
 STEP = (1e-3, 1e-6, 1e-2)
+TV_LAMBDA, TV_ITER = 1e-3, 20
 
 
 def _rank_main(rank, world, port, out):

@@ -296,3 +296,55 @@ def test_out_of_device_memory_is_reported_and_recoverable(gpu_available):
     bs.set_tilt(0, probe=c["probe"], scan_x=c["sx"], scan_y=c["sy"], measured=c["meas"], volume=c["V"])
     assert np.isfinite(bs.gradient()["grad"]).all()
     bs.close()
+
+
+def test_plain_form_gives_the_batched_results(gpu_available):
+    """mset_batch_time_plain (one launch per tilt, one CTA per position, no
+    checkpointing) leaves the same accumulated gradients as the persistent
+    batched pass (only the FP64 atomics' order differs), also when the session
+    checkpoints"""
+    tilts = [small_case(n=64, nz=6, npos=5, b=2, seed=40 + j, defocus=15.0, jitter=6.0, strength=STRENGTH)
+             for j in range(3)]
+    c0 = tilts[0]
+    bs = BatchSession(n=64, nz=6, npos=[5, 4, 5], prop=c0["prop"], sigma=c0["sigma"], potential_pixelsize=c0["dz"],
+                      slice_binning=2)
+    for j, c in enumerate(tilts):
+        k = 4 if j == 1 else 5
+        bs.set_tilt(j, probe=c["probe"], scan_x=c["sx"][:k], scan_y=c["sy"][:k], measured=c["meas"][:k],
+                    volume=c["V"])
+    bs.set_checkpoint(2)
+    ref = bs.gradient()
+    assert bs.time_plain(2) > 0
+    plain = bs.read_gradient()
+    assert bs.shape()["checkpoint"] == 2  # the session's own setting is kept
+    bs.close()
+    for key in ("grad", "probe", "posdir", "err"):
+        assert rel_l2(plain[key], ref[key]) < 1e-9, key
+
+
+@pytest.mark.parametrize("method", [MSET_MODE_MSET, MSET_MODE_SSET], ids=["mset", "sset"])
+def test_sequential_pass_on_a_cluster_equals_one_cta(gpu_available, method):
+    """run_mset with each position's 128^2 field split over an 8-CTA cluster
+    (the default where compiled) against the same pass on one CTA per field:
+    the same updates up to the order of the cluster's partial sums, and both
+    against the oracle"""
+    c = small_case(n=128, nz=6, npos=5, b=2, seed=77, defocus=20.0, jitter=4.0, strength=STRENGTH)
+    step = _steps(c, method)
+    outs = []
+    for split in (True, False):
+        with Session() as s:
+            s.set_sequential_split(split)
+            s.upload(c["V"], c["probe"], c["prop"], sigma=c["sigma"], potential_pixelsize=c["dz"], scan_x=c["sx"],
+                     scan_y=c["sy"], measured=c["meas"], step_size=step, slice_binning=c["b"])
+            assert s.sequential_split() == (8 if split else 1)
+            outs.append(s.run(method))
+    (rv1, pr1, sx1, sy1, e1), (rv0, pr0, sx0, sy0, e0) = outs
+    assert rel_l2(rv1 - c["V"], rv0 - c["V"]) < 1e-5
+    assert rel_l2(pr1 - c["probe"], pr0 - c["probe"]) < 1e-5
+    d0 = np.r_[sx0 - c["sx"], sy0 - c["sy"]]
+    assert rel_l2(np.r_[sx1 - c["sx"], sy1 - c["sy"]], d0) < coord_tol(128, np.r_[c["sx"], c["sy"]], d0)
+    assert abs(e1 - e0) <= 1e-5 * e0
+    rv_o, pr_o, _, _, _ = O.run_tilt(c["V"], c["probe"], c["prop"], c["sx"], c["sy"], c["meas"], sigma=c["sigma"],
+                                     dz=c["dz"], step=step, binning=c["b"], method=method)
+    assert rel_l2(rv1 - c["V"], rv_o - c["V"]) < TOL
+    assert rel_l2(pr1 - c["probe"], pr_o - c["probe"]) < TOL
