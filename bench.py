@@ -511,28 +511,29 @@ def large_window(args, device: int) -> dict:
 
 
 def large_iteration(args, device: int) -> dict:
-    """One batched iteration as a CUDA graph in the 256^2 window on a cubic
-    256^3 reconstruction (3 tilts x 4,096 positions, 128 slabs): rotations of
-    256^3 volumes with each shear plane over a 4-CTA cluster, the cluster
-    position kernel, TV-FISTA (lambda 1e-3 x 300).  Beam-frame volumes for
-    the data are the library's own rotations of the lab-frame volume."""
+    """One batched iteration as a CUDA graph on the large configuration's own
+    reconstruction shape (MATLAB 256 x 256 x 192, 96 slabs of 2 voxels, BF16
+    counts) on 3 of its tilts: rotations of the unequal-sided volume as
+    line transforms, the 256^2 cluster position kernel, TV-FISTA
+    (lambda 1e-3 x 300).  Beam-frame volumes for the data are the library's
+    own rotations of the lab-frame volume."""
     import torch
 
     from mset_b200 import Session, synth
     from mset_b200.batch import BatchSession
 
-    cfg = synth.CONFIGS["large_cubic_s"]
+    cfg = synth.CONFIGS["large_s"]
     spec = synth.make_specimen(cfg, per_tilt=False)
-    n, nv = cfg.window, cfg.vol[0]
-    ns = -(-nv // cfg.slice_binning)
+    n, nz = cfg.window, cfg.vol[0]
+    ns = -(-nz // cfg.slice_binning)
     npos = [spec.scan_x.size] * cfg.n_tilts
-    bs = BatchSession(n=n, nz=nv, npos=npos, prop=spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx,
+    bs = BatchSession(n=n, nz=nz, npos=npos, prop=spec.prop, sigma=spec.sigma, potential_pixelsize=cfg.dx,
                       slice_binning=cfg.slice_binning, device=device)
     bs.set_amplitude_bf16(True)
     with Session(device) as rot:
         for j, a in enumerate(spec.angles):
             bs.set_tilt(j, probe=spec.probe, scan_x=spec.scan_x, scan_y=spec.scan_y,
-                        volume=rot.rotate_volume(spec.lab, a, inverse=True))
+                        volume=synth.pad_lateral(rot.rotate_volume(spec.lab, a, inverse=True), n))
     inten = torch.from_numpy(bs.simulate()).to(f"cuda:{device}")
     g = torch.Generator(device=f"cuda:{device}")
     g.manual_seed(cfg.seed + 1000)
@@ -543,14 +544,16 @@ def large_iteration(args, device: int) -> dict:
         bs.set_tilt(j, measured=meas[off:off + npos[j]])
         off += npos[j]
     del meas
-    bs.iteration_setup(nv, spec.angles, positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter, tv_fista=True)
+    bs.iteration_setup(spec.lab.shape, spec.angles, positivity=True, tv_lambda=1e-3, tv_iter=args.tv_iter,
+                       tv_fista=True)
     bs.set_rec(0.5 * spec.lab)
     ms = bs.time_iteration(1)  # captures the graph, then one timed replay
     ms = bs.time_iteration(max(1, min(args.steps, 2)))
     units = int(bs.npos.sum()) * ns
     bs.close()
     return {"s_per_iteration": ms / 1e3, "slice_propagations_per_s": units / (ms / 1e3),
-            "workload": workload_name(cfg, ns, int(sum(npos)))}
+            "workload": workload_name(cfg, ns, int(sum(npos))) + "; reconstruction 256 x 256 x 192 (rotated as "
+                        "line transforms)"}
 
 
 def host_sample(cfg_name: str, k: int):

@@ -94,6 +94,12 @@ const char *mset_version(void);
  * patterns to the device, zero the error accumulator.  Device buffers are kept
  * and reused when the next upload has the same sizes. */
 int mset_upload(mset_session *s, const mset_upload_args *a);
+/* the same with the patterns given as a table of num_scan_pos pointers to
+ * n x n single-precision arrays (a->measured is not read): the MEX cell's
+ * own arrays, cell k = position k (column-major cell order, mex_main.cu:87
+ * borrows the cell the same way), copied to the device without a host-side
+ * gather */
+int mset_upload_cells(mset_session *s, const mset_upload_args *a, const float *const *measured_cells);
 /* 'run_mset' / 'run_sset' (mex_main.cu:98-155): one sequential pass over all
  * positions with the reference's per-position updates of RVol, probe and scan
  * positions.  Outputs (host, caller-allocated): rvol_out [nz][n][n],
@@ -165,6 +171,7 @@ int mset_sequential_split(mset_session *s);
 /* global-session shims with the MEX's lifetime (one implicit session per
  * process, recreated by every upload, mex_main.cu:13, 56) */
 int mset_mex_upload(const mset_upload_args *a);
+int mset_mex_upload_cells(const mset_upload_args *a, const float *const *measured_cells);
 int mset_mex_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out,
                  float *error_out);
 int mset_mex_error(int mode, float *error_out);
@@ -328,7 +335,14 @@ typedef struct {
 } mset_iter_args;
 
 int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a);
-/* lab-frame volume in / out: host [nv][nv][nv] float */
+/* the same for a reconstruction of any shape [nv3][nv2][nv1] (a->nv is not
+ * read): nv3 = the session's depth nz, nv1, nv2 <= n with n - nv1 and n - nv2
+ * even (laterally centred in the window), each side a rotation line length
+ * (mset_rotate_volume_nd) unless the volume is cubic; rec in / out of
+ * mset_batch_set_rec / get_rec is then [nv3][nv2][nv1] */
+int mset_batch_iteration_setup_nd(mset_session *s, const mset_iter_args *a, int nv1, int nv2, int nv3);
+/* lab-frame volume in / out: host [nv][nv][nv] float ([nv3][nv2][nv1] after
+ * mset_batch_iteration_setup_nd) */
 int mset_batch_set_rec(mset_session *s, const float *rec);
 int mset_batch_get_rec(mset_session *s, float *rec);
 /* niter iterations; err_out [niter][ntilts] (sum of (A-M)^2 of the pass before
@@ -373,6 +387,17 @@ int mset_batch_device_info(mset_session *s, void **gacc_dev, size_t *gacc_count,
  * (256: each plane split over a 4-CTA thread-block cluster). */
 int mset_rotate_volume(mset_session *s, const float *vol_in, float *vol_out, int n, const float *vec1,
                        const float *vec2, const float *vec3, double phi, double theta, double psi, int inverse);
+/* The same rotation of a volume of any shape: vol_in / vol_out host
+ * [n3][n2][n1] float (MATLAB n1 x n2 x n3), every side one of 24, 32, 48, 64,
+ * 96, 128, 160, 192, 256 (e.g. 256 x 256 x 192).  The grids, the Nyquist
+ * zeroing and the coefficient of each axis follow the reference for unequal
+ * sides (Func_rotate_3Dvol_ROTmat_FourierShear.m:70-90,
+ * SheerTransforms_for3Drot.m:16-49); each shear runs as batched 1D transforms
+ * (forward along one plane axis, phase + both directions along the other,
+ * inverse along the first). */
+int mset_rotate_volume_nd(mset_session *s, const float *vol_in, float *vol_out, int n1, int n2, int n3,
+                          const float *vec1, const float *vec2, const float *vec3, double phi, double theta,
+                          double psi, int inverse);
 
 /* ---- TV regularisation -------------------------------------------------------
  * TV_FISTA_method (fista = 1, func_lib/TV_FISTA_method.m:5-38) or TV_method

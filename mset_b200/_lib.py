@@ -44,6 +44,8 @@ SIGNATURES = {
     "mset_error": (C.c_int, [C.c_void_p, C.c_int, _F]),
     "mset_forward_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, _F, _F, _F, _F, _F]),
     "mset_adjoint_position": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _F, C.c_int, _F, _F, _F]),
+    "mset_upload_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_F)]),
+    "mset_mex_upload_cells": (C.c_int, [C.c_void_p, C.POINTER(_F)]),
     "mset_read_state": (C.c_int, [C.c_void_p, _F, _F]),
     "mset_set_sequential_split": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_sequential_split": (C.c_int, [C.c_void_p]),
@@ -68,6 +70,9 @@ SIGNATURES = {
     "mset_batch_set_amplitude_bf16": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_batch_set_checkpoint": (C.c_int, [C.c_void_p, C.c_int]),
     "mset_batch_iteration_setup": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mset_batch_iteration_setup_nd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "mset_rotate_volume_nd": (C.c_int, [C.c_void_p, _F, _F, C.c_int, C.c_int, C.c_int, _F, _F, _F, C.c_double,
+                                        C.c_double, C.c_double, C.c_int]),
     "mset_batch_set_rec": (C.c_int, [C.c_void_p, _F]),
     "mset_batch_get_rec": (C.c_int, [C.c_void_p, _F]),
     "mset_batch_iterate": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D]),

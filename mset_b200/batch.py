@@ -150,12 +150,15 @@ class BatchSession:
         check("mset_batch_set_checkpoint", self._lib.mset_batch_set_checkpoint(self._h, int(k)))
 
     # ---- full batched iteration -------------------------------------------
-    def iteration_setup(self, nv: int, angles, *, vec1=(0, 0, 1), vec2=(0, 1, 0), vec3=(1, 0, 0),
+    def iteration_setup(self, nv, angles, *, vec1=(0, 0, 1), vec2=(0, 1, 0), vec3=(1, 0, 0),
                         positivity=True, tv_lambda=0.0, tv_iter=300, tv_fista=True):
+        """nv: the cubic reconstruction's edge, or its shape (nv3, nv2, nv1)
+        (C order [nv3][nv2][nv1], nv3 = the session depth)"""
         self._angles = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1, 3))
         self._vecs = [np.ascontiguousarray(np.asarray(v, dtype=np.float32)) for v in (vec1, vec2, vec3)]
+        shape = (int(nv),) * 3 if np.isscalar(nv) else tuple(int(x) for x in nv)
         a = _lib.IterArgs()
-        a.nv = int(nv)
+        a.nv = shape[0]
         a.angles = fptr(self._angles)
         a.vec1, a.vec2, a.vec3 = (fptr(v) for v in self._vecs)
         a.use_positivity = int(bool(positivity))
@@ -163,15 +166,18 @@ class BatchSession:
         a.tv_lambda = float(tv_lambda) if tv_lambda > 0 else 1.0
         a.tv_iter = int(tv_iter)
         a.tv_fista = int(bool(tv_fista))
-        self.nv = int(nv)
-        check("mset_batch_iteration_setup", self._lib.mset_batch_iteration_setup(self._h, C.byref(a)))
+        self.rec_shape = shape
+        self.nv = shape[0]
+        nv3, nv2, nv1 = shape
+        check("mset_batch_iteration_setup_nd",
+              self._lib.mset_batch_iteration_setup_nd(self._h, C.byref(a), nv1, nv2, nv3))
 
     def set_rec(self, rec):
         r = _c32(rec)
         check("mset_batch_set_rec", self._lib.mset_batch_set_rec(self._h, fptr(r)))
 
     def get_rec(self):
-        r = np.empty((self.nv,) * 3, np.float32)
+        r = np.empty(self.rec_shape, np.float32)
         check("mset_batch_get_rec", self._lib.mset_batch_get_rec(self._h, fptr(r)))
         return r
 

@@ -137,7 +137,8 @@ struct mset_session {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // batched iteration (rotate -> pass -> rotate back -> update -> TV)
     bool it_ready = false;
-    int nv = 0;
+    int nv = 0;                  // cubic reconstruction: its edge; else 0
+    int nv1 = 0, nv2 = 0, nv3 = 0;  // reconstruction [nv3][nv2][nv1] (x fastest)
     std::vector<RotPlan> plan_inv, plan_fwd;
     DevBuf<float> rec, gvol;
     DevBuf<float> bls_rec, bls_pos;  // line search: state before the tried update
@@ -279,23 +280,31 @@ int upload_tilt_probe(mset_session *s, TiltBufs &t, const float *probe) {
     return 0;
 }
 
-int upload_tilt_measured(mset_session *s, TiltBufs &t, const float *meas) {
+// measured patterns from one contiguous [npos][n][n] buffer, or (cells != NULL)
+// from a table of npos pointers to n x n patterns: the MEX cell's own arrays,
+// as the reference borrows them (mex_main.cu:87), with no host-side gather
+int upload_tilt_measured(mset_session *s, TiltBufs &t, const float *meas, const float *const *cells = nullptr) {
     const size_t n2 = (size_t)s->n * s->n;
     const size_t cnt = n2 * t.npos;
     if (cnt == 0) return 0;
     // intensities are square-rooted in the loss: a negative, NaN or infinite
     // count would turn every gradient of the pass into NaN
-    size_t bad = cnt;
-    for (size_t i = 0; i < cnt; ++i)
-        if (!(meas[i] >= 0.f) || meas[i] == INFINITY) {
-            bad = i;
-            break;
-        }
-    if (bad < cnt)
-        return fail(MSET_E_ARG, "measured pattern %zu has a negative, NaN or infinite value at pixel %zu (%g)",
-                    bad / n2, bad % n2, (double)meas[bad]);
+    for (int p = 0; p < t.npos; ++p) {
+        const float *m = cells ? cells[p] : meas + (size_t)p * n2;
+        if (!m) return fail(MSET_E_ARG, "measured pattern %d is a null pointer", p);
+        for (size_t i = 0; i < n2; ++i)
+            if (!(m[i] >= 0.f) || m[i] == INFINITY)
+                return fail(MSET_E_ARG, "measured pattern %d has a negative, NaN or infinite value at pixel %zu (%g)",
+                            p, i, (double)m[i]);
+    }
     CK(s->meas_tmp.ensure(std::max(s->meas_tmp.n, cnt)));
-    CK(cudaMemcpyAsync(s->meas_tmp.p, meas, sizeof(float) * cnt, cudaMemcpyHostToDevice, s->st));
+    if (cells) {
+        for (int p = 0; p < t.npos; ++p)
+            CK(cudaMemcpyAsync(s->meas_tmp.p + (size_t)p * n2, cells[p], sizeof(float) * n2, cudaMemcpyHostToDevice,
+                               s->st));
+    } else {
+        CK(cudaMemcpyAsync(s->meas_tmp.p, meas, sizeof(float) * cnt, cudaMemcpyHostToDevice, s->st));
+    }
     if (s->batch && s->amp_bf16) {
         t.amp.release();
         CK(t.ampb.ensure(cnt));
@@ -483,10 +492,10 @@ int mset_destroy(mset_session *s) {
     return 0;
 }
 
-int mset_upload(mset_session *s, const mset_upload_args *a) {
+static int upload_impl(mset_session *s, const mset_upload_args *a, const float *const *cells) {
     if (!s || !a) return fail(MSET_E_ARG, "null argument");
     if (!a->RVol || !a->init_wave2D || !a->prop2D || (!a->scan_xlist && a->num_scan_pos) ||
-        (!a->scan_ylist && a->num_scan_pos) || (!a->measured && a->num_scan_pos))
+        (!a->scan_ylist && a->num_scan_pos) || (!a->measured && !cells && a->num_scan_pos))
         return fail(MSET_E_ARG, "null array in upload arguments");
     if (a->num_scan_pos < 0) return fail(MSET_E_ARG, "num_scan_pos < 0");
     if (a->N_scan_x <= 0 || a->N_scan_y <= 0) return fail(MSET_E_ARG, "N_scan_x and N_scan_y must be positive");
@@ -521,7 +530,7 @@ int mset_upload(mset_session *s, const mset_upload_args *a) {
         CK(cudaMemcpyAsync(t.sx.p, a->scan_xlist, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
         CK(cudaMemcpyAsync(t.sy.p, a->scan_ylist, sizeof(float) * t.npos, cudaMemcpyHostToDevice, s->st));
     }
-    rc = upload_tilt_measured(s, t, a->measured);
+    rc = upload_tilt_measured(s, t, a->measured, cells);
     if (rc) return rc;
     // work list for the forward-only pass
     std::vector<int2> it(std::max(1, t.npos));
@@ -532,6 +541,13 @@ int mset_upload(mset_session *s, const mset_upload_args *a) {
     CK(cudaStreamSynchronize(s->st));
     s->ready = true;
     return 0;
+}
+
+int mset_upload(mset_session *s, const mset_upload_args *a) { return upload_impl(s, a, nullptr); }
+
+int mset_upload_cells(mset_session *s, const mset_upload_args *a, const float *const *measured_cells) {
+    if (!measured_cells && a && a->num_scan_pos) return fail(MSET_E_ARG, "null pattern table");
+    return upload_impl(s, a, measured_cells);
 }
 
 int mset_run_ex(mset_session *s, int mode, int adjoint, float *rvol_out, float *probe_out, float *scan_x_out,
@@ -769,6 +785,13 @@ int mset_mex_upload(const mset_upload_args *a) {
         if (rc) return rc;
     }
     return mset_upload(g_mex, a);
+}
+int mset_mex_upload_cells(const mset_upload_args *a, const float *const *measured_cells) {
+    if (!g_mex) {
+        int rc = mset_create(0, &g_mex);
+        if (rc) return rc;
+    }
+    return mset_upload_cells(g_mex, a, measured_cells);
 }
 int mset_mex_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out, float *scan_y_out, float *error_out) {
     if (!g_mex) return fail(MSET_E_STATE, "run called before upload");
@@ -1091,13 +1114,26 @@ int mset_batch_time(mset_session *s, int reps, double *ms_per_pass) {
 }
 
 // ---- Fourier-shear rotation -------------------------------------------------
+// work buffers of a rotation of an n1 x n2 x n3 volume: a cubic one rotates
+// plane by plane (k_shear), any other shape line by line (rot_apply3)
+static int rot_prepare3(mset_session *s, int n1, int n2, int n3) {
+    if (n1 == n2 && n2 == n3) {
+        if (!rot_supported(n1))
+            return fail(MSET_E_UNSUPPORTED, "rotation of a %d^3 volume has no compiled kernel "
+                                            "(supported: 24, 32, 48, 64, 96, 128, 160, 256)", n1);
+    } else if (!rot_line_supported(n1) || !rot_line_supported(n2) || !rot_line_supported(n3)) {
+        return fail(MSET_E_UNSUPPORTED, "rotation of a %d x %d x %d volume: every side must be one of 24, 32, 48, "
+                                        "64, 96, 128, 160, 192, 256", n1, n2, n3);
+    }
+    const size_t nvox = (size_t)n1 * n2 * n3;
+    CK(s->rot_vol.ensure(std::max(s->rot_vol.n, nvox)));
+    CK(s->rot_S.ensure(std::max(s->rot_S.n, nvox)));
+    return 0;
+}
+
 static int rot_prepare(mset_session *s, int n) {
-    if (!rot_supported(n))
-        return fail(MSET_E_UNSUPPORTED, "rotation of a %d^3 volume has no compiled kernel "
-                                        "(supported: 24, 32, 48, 64, 96, 128, 160, 256)", n);
-    const size_t n3 = (size_t)n * n * n;
-    CK(s->rot_vol.ensure(n3));
-    CK(s->rot_S.ensure(n3));
+    int rc = rot_prepare3(s, n, n, n);
+    if (rc) return rc;
     if (s->rot_n != n) {
         std::vector<float2> h;
         rot_twiddles(n, h);
@@ -1106,6 +1142,37 @@ static int rot_prepare(mset_session *s, int n) {
         CK(cudaStreamSynchronize(s->st));
         s->rot_n = n;
     }
+    return 0;
+}
+
+// rotation of the reconstruction-shaped volume src into dst (may alias)
+static int rotate_rec(mset_session *s, const RotPlan &pl, const float *src, float *dst) {
+    if (s->nv > 0) return rot_apply(pl, s->nv, src, dst, s->rot_S.p, s->rot_tw.p, s->sms, s->st);
+    return rot_apply3(pl, s->nv1, s->nv2, s->nv3, src, dst, s->rot_S.p, s->sms, s->st);
+}
+
+int mset_rotate_volume_nd(mset_session *s, const float *vol_in, float *vol_out, int n1, int n2, int n3,
+                          const float *vec1, const float *vec2, const float *vec3, double phi, double theta,
+                          double psi, int inverse) {
+    Range range_("mset_rotate_volume_nd");
+    if (!s || !vol_in || !vol_out || !vec1 || !vec2 || !vec3) return fail(MSET_E_ARG, "null argument");
+    if (n1 <= 1 || n2 <= 1 || n3 <= 1) return fail(MSET_E_ARG, "bad volume size %d x %d x %d", n1, n2, n3);
+    int rc = set_device(s);
+    if (rc) return rc;
+    if (!rot_line_supported(n1) || !rot_line_supported(n2) || !rot_line_supported(n3))
+        return fail(MSET_E_UNSUPPORTED, "rotation of a %d x %d x %d volume: every side must be one of 24, 32, 48, "
+                                        "64, 96, 128, 160, 192, 256", n1, n2, n3);
+    const size_t nvox = (size_t)n1 * n2 * n3;
+    CK(s->rot_vol.ensure(std::max(s->rot_vol.n, nvox)));
+    CK(s->rot_S.ensure(std::max(s->rot_S.n, nvox)));
+    const double v1[3] = {vec1[0], vec1[1], vec1[2]}, v2[3] = {vec2[0], vec2[1], vec2[2]},
+                 v3[3] = {vec3[0], vec3[1], vec3[2]};
+    RotPlan pl;
+    rot_plan(v1, v2, v3, phi, theta, psi, inverse != 0, &pl);
+    CK(cudaMemcpyAsync(s->rot_vol.p, vol_in, sizeof(float) * nvox, cudaMemcpyHostToDevice, s->st));
+    CKL(rot_apply3(pl, n1, n2, n3, s->rot_vol.p, s->rot_vol.p, s->rot_S.p, s->sms, s->st), "rotation");
+    CK(cudaMemcpyAsync(vol_out, s->rot_vol.p, sizeof(float) * nvox, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
     return 0;
 }
 
@@ -1188,16 +1255,19 @@ __global__ void k_record_err(const double *err, int J, double *hist, int cap, un
 }
 }  // namespace
 
-int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
+int mset_batch_iteration_setup_nd(mset_session *s, const mset_iter_args *a, int nv1, int nv2, int nv3) {
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!a || !a->angles || !a->vec1 || !a->vec2 || !a->vec3) return fail(MSET_E_ARG, "null argument");
-    const int nv = a->nv;
-    if (nv != s->nz) return fail(MSET_E_ARG, "the reconstruction edge nv (%d) must equal the depth nz (%d)", nv, s->nz);
-    if (nv > s->n) return fail(MSET_E_ARG, "the reconstruction edge nv (%d) exceeds the window (%d)", nv, s->n);
-    if ((s->n - nv) % 2) return fail(MSET_E_ARG, "window minus volume edge must be even (centred padding)");
+    if (nv3 != s->nz)
+        return fail(MSET_E_ARG, "the reconstruction depth nv3 (%d) must equal the session depth nz (%d)", nv3, s->nz);
+    if (nv1 > s->n || nv2 > s->n)
+        return fail(MSET_E_ARG, "the reconstruction (%d x %d laterally) exceeds the window (%d)", nv1, nv2, s->n);
+    if ((s->n - nv1) % 2 || (s->n - nv2) % 2)
+        return fail(MSET_E_ARG, "window minus volume sides must be even (centred padding)");
     if (a->use_tv && (!(a->tv_lambda > 0) || a->tv_iter < 0)) return fail(MSET_E_ARG, "bad TV parameters");
-    rc = rot_prepare(s, nv);
+    const bool cubic = nv1 == nv2 && nv2 == nv3;
+    rc = cubic ? rot_prepare(s, nv1) : rot_prepare3(s, nv1, nv2, nv3);
     if (rc) return rc;
     const int J = (int)s->tilts.size();
     const double v1[3] = {a->vec1[0], a->vec1[1], a->vec1[2]}, v2[3] = {a->vec2[0], a->vec2[1], a->vec2[2]},
@@ -1209,7 +1279,7 @@ int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
         rot_plan(v1, v2, v3, an[0], an[1], an[2], true, &s->plan_inv[j]);   // Func_inv_rot (STEP01_ROTATION.m:13)
         rot_plan(v1, v2, v3, an[0], an[1], an[2], false, &s->plan_fwd[j]);  // Func_rot (Run_MSET_recon.m:179)
     }
-    const size_t V = (size_t)nv * nv * nv;
+    const size_t V = (size_t)nv1 * nv2 * nv3;
     CK(s->rec.ensure(V));
     CK(s->gvol.ensure(V));
     CK(s->gacc.ensure(V));
@@ -1217,7 +1287,10 @@ int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
     CK(s->mx_bits.ensure(1));
     CK(s->mx.ensure(1));
     CK(cudaMemsetAsync(s->rec.p, 0, sizeof(float) * V, s->st));
-    s->nv = nv;
+    s->nv = cubic ? nv1 : 0;
+    s->nv1 = nv1;
+    s->nv2 = nv2;
+    s->nv3 = nv3;
     s->it_pos = a->use_positivity ? 1 : 0;
     s->it_tv = a->use_tv ? 1 : 0;
     s->it_tv_iter = a->tv_iter;
@@ -1237,12 +1310,17 @@ int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
     return 0;
 }
 
+int mset_batch_iteration_setup(mset_session *s, const mset_iter_args *a) {
+    if (!a) return fail(MSET_E_ARG, "null argument");
+    return mset_batch_iteration_setup_nd(s, a, a->nv, a->nv, a->nv);
+}
+
 int mset_batch_set_rec(mset_session *s, const float *rec) {
     int rc = batch_ok(s);
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
     if (!rec) return fail(MSET_E_ARG, "null volume");
-    CK(cudaMemcpyAsync(s->rec.p, rec, sizeof(float) * (size_t)s->nv * s->nv * s->nv, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->rec.p, rec, sizeof(float) * (size_t)s->nv1 * s->nv2 * s->nv3, cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
     return 0;
 }
@@ -1252,7 +1330,7 @@ int mset_batch_get_rec(mset_session *s, float *rec) {
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
     if (!rec) return fail(MSET_E_ARG, "null volume");
-    CK(cudaMemcpyAsync(rec, s->rec.p, sizeof(float) * (size_t)s->nv * s->nv * s->nv, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(rec, s->rec.p, sizeof(float) * (size_t)s->nv1 * s->nv2 * s->nv3, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     return 0;
 }
@@ -1264,16 +1342,16 @@ int mset_batch_get_rec(mset_session *s, float *rec) {
 // shards tilts over GPUs all-reduces gacc between the phases.
 static int record_phase(mset_session *s, int phase, bool with_tv = true, bool with_hist = true) {
     const int J = (int)s->tilts.size();
-    const int nv = s->nv, n = s->n;
-    const long V = (long)nv * nv * nv;
+    const int n = s->n;
+    const long V = (long)s->nv1 * s->nv2 * s->nv3;
     const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
     const int bvox = s->method == MSET_MODE_SSET ? s->nz : s->b;
     const size_t n2 = (size_t)n * n;
     if (phase == 2) goto update;
     // 1. beam-frame volumes V_j = pad(Func_inv_rot(rec, angles_j))
     for (int j = 0; j < J; ++j) {
-        CKL(rot_apply(s->plan_inv[j], nv, s->rec.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
-        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, nv, n, s->st), "pad");
+        CKL(rotate_rec(s, s->plan_inv[j], s->rec.p, s->gvol.p), "rotation");
+        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, s->nv1, s->nv2, s->nv3, n, s->st), "pad");
     }
     // 2. the batched pass over all positions of all tilts
     for (auto &t : s->tilts) {
@@ -1290,8 +1368,9 @@ static int record_phase(mset_session *s, int phase, bool with_tv = true, bool wi
     }
     // 3. gradient back to the lab frame: sum_j Func_rot(G_j)
     for (int j = 0; j < J; ++j) {
-        CKL(vol_slab_to_volume(s->tilts[j].grad.p, s->gvol.p, nv, n, bvox, s->st), "slab_to_volume");
-        CKL(rot_apply(s->plan_fwd[j], nv, s->gvol.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
+        CKL(vol_slab_to_volume(s->tilts[j].grad.p, s->gvol.p, s->nv1, s->nv2, s->nv3, n, bvox, s->st),
+            "slab_to_volume");
+        CKL(rotate_rec(s, s->plan_fwd[j], s->gvol.p, s->gvol.p), "rotation");
         CKL(vol_accumulate(s->gvol.p, s->gacc.p, V, j == 0, s->st), "accumulate");
     }
     if (phase == 1) return 0;
@@ -1303,8 +1382,8 @@ update:
         CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
         CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
         CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
-        const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
-                  s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
+        const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, s->nv1, s->nv2, s->nv3,
+                        s->it_tv_lambda, s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
         CKL(tv_prox(ta, s->st), "tv");
         CKL(vol_mul(s->tv_out.p, s->rec.p, V, s->mx.p, s->st), "rescale");
     }
@@ -1375,13 +1454,12 @@ int mset_batch_iterate(mset_session *s, int niter, int use_graph, double *err_ou
 
 // TV / TV-FISTA of rec / max(rec), rescaled by max(rec) (Run_MSET_recon.m:267-270)
 static int record_tv(mset_session *s) {
-    const int nv = s->nv;
-    const long V = (long)nv * nv * nv;
+    const long V = (long)s->nv1 * s->nv2 * s->nv3;
     CKL(vol_max(s->rec.p, V, s->mx_bits.p, s->mx.p, s->st), "max");
     CKL(vol_scale(s->rec.p, s->tv_in.p, V, s->mx.p, s->st), "scale");
     CK(cudaMemsetAsync(s->tv_err.p, 0, sizeof(double), s->st));
-    const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, nv, nv, nv, s->it_tv_lambda,
-                    s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
+    const TvArgs ta{s->tv_in.p, s->tv_out.p, s->tv_P.p, s->tv_Y.p, s->tv_D.p, s->nv1, s->nv2, s->nv3,
+                    s->it_tv_lambda, s->it_tv_iter, s->it_tv_fista, s->tv_err.p};
     CKL(tv_prox(ta, s->st), "tv");
     CKL(vol_mul(s->tv_out.p, s->rec.p, V, s->mx.p, s->st), "rescale");
     return 0;
@@ -1391,12 +1469,12 @@ static int record_tv(mset_session *s) {
 // forward only (run_error_mset, mset.cu:557-696), sums into s->err
 static int record_error_phase(mset_session *s) {
     const int J = (int)s->tilts.size();
-    const int nv = s->nv, n = s->n;
+    const int n = s->n;
     const int nsg = s->method == MSET_MODE_SSET ? 1 : s->ns;
     const int bvox = s->method == MSET_MODE_SSET ? s->nz : s->b;
     for (int j = 0; j < J; ++j) {
-        CKL(rot_apply(s->plan_inv[j], nv, s->rec.p, s->gvol.p, s->rot_S.p, s->rot_tw.p, s->sms, s->st), "rotation");
-        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, nv, n, s->st), "pad");
+        CKL(rotate_rec(s, s->plan_inv[j], s->rec.p, s->gvol.p), "rotation");
+        CKL(vol_pad(s->gvol.p, s->tilts[j].V.p, s->nv1, s->nv2, s->nv3, n, s->st), "pad");
     }
     CK(cudaMemsetAsync(s->err.p, 0, sizeof(double) * J, s->st));
     CKL(launch_transmission(s->d_tilts.p, J, n, s->nz, bvox, nsg, s->sigma * s->dz, s->st), "transmission");
@@ -1409,7 +1487,7 @@ static int record_error_phase(mset_session *s) {
 // copy of the state a line-search step may have to undo: rec, probes, positions
 static int bls_state(mset_session *s, bool save) {
     const size_t n2 = (size_t)s->n * s->n;
-    const long V = (long)s->nv * s->nv * s->nv;
+    const long V = (long)s->nv1 * s->nv2 * s->nv3;
     if (save) CK(cudaMemcpyAsync(s->bls_rec.p, s->rec.p, sizeof(float) * V, cudaMemcpyDeviceToDevice, s->st));
     else CK(cudaMemcpyAsync(s->rec.p, s->bls_rec.p, sizeof(float) * V, cudaMemcpyDeviceToDevice, s->st));
     for (size_t j = 0; j < s->tilts.size(); ++j) {
@@ -1454,7 +1532,7 @@ int mset_batch_iterate_bls(mset_session *s, int niter, double bls_parameter, dou
     if (iters_out) *iters_out = 0;
     const int J = (int)s->tilts.size();
     const size_t n2 = (size_t)s->n * s->n;
-    const long V = (long)s->nv * s->nv * s->nv;
+    const long V = (long)s->nv1 * s->nv2 * s->nv3;
     const int grid = persistent_grid(s, std::max(1, s->total_pos));
     rc = ensure_save(s, grid);
     if (rc) return rc;
@@ -1565,7 +1643,7 @@ int mset_batch_device_info(mset_session *s, void **gacc_dev, size_t *gacc_count,
     if (rc) return rc;
     if (!s->it_ready) return fail(MSET_E_STATE, "mset_batch_iteration_setup first");
     if (gacc_dev) *gacc_dev = s->gacc.p;
-    if (gacc_count) *gacc_count = (size_t)s->nv * s->nv * s->nv;
+    if (gacc_count) *gacc_count = (size_t)s->nv1 * s->nv2 * s->nv3;
     if (stream) *stream = (void *)s->st;
     if (err_dev) *err_dev = s->err.p;
     return 0;

@@ -229,6 +229,275 @@ static int shear(int n, float2 *S, const float2 *twn, int dim, double a, double 
 }
 
 // ---------------------------------------------------------------------------
+// volumes of any shape n1 x n2 x n3: every shear as batched 1D transforms
+// ---------------------------------------------------------------------------
+// A shear along axis d multiplies the 2D spectrum of each plane (axes a, b)
+// by exp(i 2 pi g_d (c_a g_a + c_b g_b) / n_d), or by 1 where any of the
+// three grids is at its Nyquist index (SheerTransforms_for3Drot.m:29-49 with
+// the grids of Func_rotate_3Dvol_ROTmat_FourierShear.m:70-90).  For planes of
+// unequal sides this is done line by line through global memory:
+//   (1) forward transform of every line along a (natural -> scrambled),
+//   (2) along b: forward transform, the phase (a's frequency from the line's
+//       scrambled position, d's grid from its index), inverse transform,
+//   (3) inverse transform along a (scrambled -> natural), real() fused into
+//       the fourth shear of a sub-step.
+// Each kernel reads and writes the complex volume once; a CTA transforms a
+// batch of ROWS lines in shared memory with the radix passes of the position
+// kernel.  Lines are batched along the other axis of smallest stride, so
+// every global access is coalesced.
+
+// ROWS lines of length L in one CTA's shared memory
+template <int L_, int R1_, int ROWS_>
+struct LineGeo : Geo<L_, R1_, 256> {
+    static constexpr int ROWS = ROWS_;
+    static constexpr int FIELD = ROWS_ * Geo<L_, R1_, 256>::S;
+};
+
+// the lines of one transform axis: a = transform axis, p = the other axis of
+// smaller stride (batched), q = the remaining one
+struct LineMap {
+    long sa, sp, sq;
+    int La, np, nq;
+    int pa_is_a;  // shift kernel: 1 if p is the first-transformed axis, 0 if p is the shear axis
+};
+
+// the grid value of a frequency index (rot_grid_val) and whether it is Nyquist
+__device__ __forceinline__ int grid_of(int k, int n, bool *nyq) { return rot_grid_val(k, n, nyq); }
+
+// MODE 0: forward along the axis (natural -> scrambled); 1: inverse (scrambled
+// -> natural, REAL keeps the real part); 2: the shift: forward, phase,
+// inverse.  For MODE 2 the lines run along b; (ra1, La_a) give the scrambled
+// layout of the first-transformed axis a; nd is the shear axis length; c_a,
+// c_b the shear coefficients of a and b.
+template <class LG, int MODE, bool REAL>
+__global__ void __launch_bounds__(256) k_line(float2 *S, LineMap m, int ra1, int La_a, int nd, double c_a,
+                                              double c_b, float scale) {
+    constexpr int L = LG::N, R1 = LG::R1, ROWS = LG::ROWS, NT = LG::NT;
+    extern __shared__ __align__(16) float2 sm[];
+    float2 *buf = sm;
+    float2 *tw = buf + LG::FIELD;
+    __shared__ double s_row[ROWS];  // per row: 2 g_d c_a g_a / n_d (MODE 2)
+    __shared__ double s_gd[ROWS];   // per row: 2 g_d / n_d, or NaN on a Nyquist plane
+    for (int i = threadIdx.x; i < L; i += NT) {
+        const int k2 = i / R1, n1 = i % R1;
+        const long mm = (long)n1 * k2 % L;
+        double sn, cs;
+        sincospi(-2.0 * (double)mm / (double)L, &sn, &cs);
+        tw[i] = make_float2((float)cs, (float)sn);
+    }
+    const int nbp = (m.np + ROWS - 1) / ROWS;
+    const long batches = (long)nbp * m.nq;
+    for (long bt = blockIdx.x; bt < batches; bt += gridDim.x) {
+        const int bp = (int)(bt % nbp), iq = (int)(bt / nbp);
+        __syncthreads();
+        if (MODE == 2 && threadIdx.x < ROWS) {
+            const int ip = bp * ROWS + threadIdx.x;
+            // the line's position along a (scrambled) and its index along d
+            const int la = m.pa_is_a ? ip : iq, id = m.pa_is_a ? iq : ip;
+            const int ka = la / ra1 + (La_a / ra1) * (la % ra1);
+            bool qa, qd;
+            const int ga = grid_of(ka, La_a, &qa), gd = grid_of(id, nd, &qd);
+            s_gd[threadIdx.x] = (qa || qd) ? NAN : 2.0 * (double)gd / (double)nd;
+            s_row[threadIdx.x] = 2.0 * (double)gd * c_a * (double)ga / (double)nd;
+        }
+        // load the batch (coalesced: along the line when it is contiguous, else across lines)
+        for (int i = threadIdx.x; i < ROWS * L; i += NT) {
+            int r, k;
+            if (m.sa == 1) {
+                r = i / L;
+                k = i % L;
+            } else {
+                r = i % ROWS;
+                k = i / ROWS;
+            }
+            const int ip = bp * ROWS + r;
+            buf[LG::at(r, k)] = ip < m.np ? S[(long)ip * m.sp + (long)iq * m.sq + (long)k * m.sa] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        if constexpr (MODE == 0 || MODE == 2) {
+            row_passA<LG, 0, -1>(buf, tw, NoOp{});
+            sync_rows();
+            row_passB<LG, -1>(buf);
+        }
+        if constexpr (MODE == 2) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < ROWS * L; i += NT) {
+                const int r = i / L, lb = i % L;
+                const double gdn = s_gd[r];
+                float2 f = make_float2(scale, 0.f);
+                bool qb;
+                const int gb = grid_of(LG::scr(lb), L, &qb);
+                if (!qb && !isnan(gdn)) {
+                    double t = s_row[r] + gdn * c_b * (double)gb;  // phase / pi
+                    t -= 2.0 * rint(0.5 * t);                        // into [-1, 1]
+                    float sn, cs;
+                    sincospif((float)t, &sn, &cs);
+                    f = make_float2(scale * cs, scale * sn);
+                }
+                float2 &v = buf[LG::at(r, lb)];
+                v = cmul(v, f);
+            }
+            __syncthreads();
+        }
+        if constexpr (MODE == 1 || MODE == 2) {
+            row_passB<LG, +1>(buf);
+            sync_rows();
+            row_passA<LG, +1, 0>(buf, tw, NoOp{});
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < ROWS * L; i += NT) {
+            int r, k;
+            if (m.sa == 1) {
+                r = i / L;
+                k = i % L;
+            } else {
+                r = i % ROWS;
+                k = i / ROWS;
+            }
+            const int ip = bp * ROWS + r;
+            if (ip < m.np) {
+                float2 v = buf[LG::at(r, k)];
+                if (REAL) v.y = 0.f;
+                S[(long)ip * m.sp + (long)iq * m.sq + (long)k * m.sa] = v;
+            }
+        }
+    }
+}
+
+// one geometry per supported line length (256 threads, radix split L = R1 R2)
+#define MSET_LINE_GEOS(X) \
+    X(24, 8, 32) X(32, 8, 32) X(48, 16, 16) X(64, 8, 32) X(96, 16, 16) X(128, 16, 16) X(160, 16, 16) \
+    X(192, 16, 16) X(256, 16, 16)
+
+bool rot_line_supported(int n) {
+#define X(L_, R1_, ROWS_) \
+    if (n == L_) return true;
+    MSET_LINE_GEOS(X)
+#undef X
+    return false;
+}
+
+static int line_r1(int n) {
+#define X(L_, R1_, ROWS_) \
+    if (n == L_) return R1_;
+    MSET_LINE_GEOS(X)
+#undef X
+    return 0;
+}
+
+template <class LG, int MODE, bool REAL>
+static int launch_line_k(float2 *S, const LineMap &m, int ra1, int La_a, int nd, double c_a, double c_b, float scale,
+                         int sms, cudaStream_t st) {
+    auto k = k_line<LG, MODE, REAL>;
+    const size_t sm = sizeof(float2) * ((size_t)LG::FIELD + LG::N);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return (int)e;
+    const long batches = (long)((m.np + LG::ROWS - 1) / LG::ROWS) * m.nq;
+    const int grid = (int)std::min<long>(batches, (long)sms * 8);
+    k<<<grid, 256, sm, st>>>(S, m, ra1, La_a, nd, c_a, c_b, scale);
+    return (int)cudaGetLastError();
+}
+
+static int launch_line(int mode, bool real, float2 *S, const LineMap &m, int ra1, int La_a, int nd, double c_a,
+                       double c_b, float scale, int sms, cudaStream_t st) {
+#define X(L_, R1_, ROWS_)                                                                                    \
+    if (m.La == L_) {                                                                                        \
+        using LG = LineGeo<L_, R1_, ROWS_>;                                                                  \
+        if (mode == 0) return launch_line_k<LG, 0, false>(S, m, ra1, La_a, nd, c_a, c_b, scale, sms, st);    \
+        if (mode == 2) return launch_line_k<LG, 2, false>(S, m, ra1, La_a, nd, c_a, c_b, scale, sms, st);    \
+        if (real) return launch_line_k<LG, 1, true>(S, m, ra1, La_a, nd, c_a, c_b, scale, sms, st);          \
+        return launch_line_k<LG, 1, false>(S, m, ra1, La_a, nd, c_a, c_b, scale, sms, st);                   \
+    }
+    MSET_LINE_GEOS(X)
+#undef X
+    return (int)cudaErrorInvalidValue;
+}
+
+// lines along axis `ax` (0-based: 0 = x fastest) of an n[0] x n[1] x n[2]
+// volume; p = the other axis of smaller stride
+static LineMap line_map(const int n[3], int ax) {
+    const long st[3] = {1, n[0], (long)n[0] * n[1]};
+    int o[2], c = 0;
+    for (int i = 0; i < 3; ++i)
+        if (i != ax) o[c++] = i;  // o[0] has the smaller stride
+    LineMap m;
+    m.sa = st[ax];
+    m.La = n[ax];
+    m.sp = st[o[0]];
+    m.np = n[o[0]];
+    m.sq = st[o[1]];
+    m.nq = n[o[1]];
+    m.pa_is_a = 0;
+    return m;
+}
+
+// one shear along MATLAB dimension dim (1, 2, 3) of an n1 x n2 x n3 complex volume
+static int shear_lines(const int n[3], float2 *S, int dim, double ca, double cb, bool real, int sms, cudaStream_t st) {
+    const int d = dim - 1;
+    // the two transformed axes and their coefficients
+    // (dim 1: axis 2 <-> a, axis 3 <-> b; dim 2: axis 1 <-> b, axis 3 <-> a;
+    //  dim 3: axis 1 <-> a, axis 2 <-> b: SheerTransforms_for3Drot.m:16-49)
+    int ax0, ax1;
+    double c0, c1;
+    if (d == 0) {
+        ax0 = 1; c0 = ca; ax1 = 2; c1 = cb;
+    } else if (d == 1) {
+        ax0 = 0; c0 = cb; ax1 = 2; c1 = ca;
+    } else {
+        ax0 = 0; c0 = ca; ax1 = 1; c1 = cb;
+    }
+    // first-transformed axis: ax0; the shift runs along ax1
+    const LineMap ma = line_map(n, ax0);
+    LineMap mb = line_map(n, ax1);
+    // along ax1 the other two axes are ax0 and d: which one is batched (p)?
+    mb.pa_is_a = (mb.sp == (ax0 == 0 ? 1 : ax0 == 1 ? (long)n[0] : (long)n[0] * n[1])) ? 1 : 0;
+    const int ra1 = line_r1(n[ax0]);
+    const float scale = 1.0f / ((float)n[ax0] * (float)n[ax1]);
+    int rc = launch_line(0, false, S, ma, 0, 0, 0, 0, 0, 1.f, sms, st);
+    if (!rc) rc = launch_line(2, false, S, mb, ra1, n[ax0], n[d], c0, c1, scale, sms, st);
+    if (!rc) rc = launch_line(1, real, S, ma, 0, 0, 0, 0, 0, 1.f, sms, st);
+    return rc;
+}
+
+// complex S = ifftshift(real vol) / out = fftshift(real(S)) for n1 x n2 x n3
+__global__ void k_rot_pre3(const float *vol, float2 *S, int n1, int n2, int n3) {
+    const long n12 = (long)n1 * n2, total = n12 * n3;
+    const int h1 = (n1 + 1) / 2, h2 = (n2 + 1) / 2, h3 = (n3 + 1) / 2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int i3 = (int)(i / n12), i2 = (int)((i / n1) % n2), i1 = (int)(i % n1);
+        S[(long)((i3 + h3) % n3) * n12 + (long)((i2 + h2) % n2) * n1 + (i1 + h1) % n1] = make_float2(vol[i], 0.f);
+    }
+}
+__global__ void k_rot_post3(const float2 *S, float *out, int n1, int n2, int n3) {
+    const long n12 = (long)n1 * n2, total = n12 * n3;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int i3 = (int)(i / n12), i2 = (int)((i / n1) % n2), i1 = (int)(i % n1);
+        out[(long)((i3 + n3 / 2) % n3) * n12 + (long)((i2 + n2 / 2) % n2) * n1 + (i1 + n1 / 2) % n1] = S[i].x;
+    }
+}
+
+int rot_apply3(const RotPlan &pl, int n1, int n2, int n3, const float *vol, float *out, float2 *S, int sms,
+               cudaStream_t st) {
+    const long total = (long)n1 * n2 * n3;
+    if (!pl.active) {
+        if (out != vol) return (int)cudaMemcpyAsync(out, vol, sizeof(float) * total, cudaMemcpyDeviceToDevice, st);
+        return 0;
+    }
+    const int n[3] = {n1, n2, n3};
+    const int g = (int)std::min<long>((total + 255) / 256, (long)sms * 8);
+    k_rot_pre3<<<g, 256, 0, st>>>(vol, S, n1, n2, n3);
+    int rc = (int)cudaGetLastError();
+    if (rc) return rc;
+    for (int s = 0; s < pl.num_step; ++s)
+        for (int k = 0; k < 4; ++k) {
+            rc = shear_lines(n, S, pl.dim[k], pl.a[k], pl.b[k], k == 3, sms, st);
+            if (rc) return rc;
+        }
+    k_rot_post3<<<g, 256, 0, st>>>(S, out, n1, n2, n3);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // host-side rotation plan (double precision), restating the reference
 // ---------------------------------------------------------------------------
 namespace {

@@ -1,4 +1,4 @@
-// mset_rotate.cuh -- Fourier-shear rotation of cubic volumes (mset_rotate.cu)
+// mset_rotate.cuh -- Fourier-shear rotation of volumes (mset_rotate.cu)
 #pragma once
 #include <cuda_runtime.h>
 #include <vector>
@@ -21,5 +21,10 @@ int rot_twiddles(int n, std::vector<float2> &h);
 // out = rotation of vol (device, [n][n][n]); S: n^3 complex work buffer
 int rot_apply(const RotPlan &pl, int n, const float *vol, float *out, float2 *S, const float2 *twn, int sms,
               cudaStream_t st);
+// any shape [n3][n2][n1] (every side a supported line length): each shear as
+// batched 1D transforms; S: n1 n2 n3 complex work buffer
+bool rot_line_supported(int n);
+int rot_apply3(const RotPlan &pl, int n1, int n2, int n3, const float *vol, float *out, float2 *S, int sms,
+               cudaStream_t st);
 
 }  // namespace mset

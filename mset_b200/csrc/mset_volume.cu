@@ -131,24 +131,25 @@ __global__ void k_positivity(float *v, long n) {
 // beam-frame volume of a tilt: V[z][y][x] (n x n window) = centred copy of
 // the rotated nv^3 volume (zero elsewhere): the volume zero-padded laterally
 // to the probe window (exact under the periodic multislice: V = 0 gives T = 1)
-__global__ void k_pad(const float *src, float *V, int nv, int n) {
-    const long nn = (long)n * n, total = nn * nv;
-    const int o = (n - nv) / 2;
+// beam-frame volume [n3][n2][n1] centred in the n x n window: V [n3][n][n]
+__global__ void k_pad(const float *src, float *V, int n1, int n2, int n3, int n) {
+    const long nn = (long)n * n, total = nn * n3;
+    const int o1 = (n - n1) / 2, o2 = (n - n2) / 2;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int z = (int)(i / nn), y = (int)((i / n) % n), x = (int)(i % n);
-        const int yy = y - o, xx = x - o;
-        V[i] = (yy >= 0 && yy < nv && xx >= 0 && xx < nv) ? src[((long)z * nv + yy) * nv + xx] : 0.f;
+        const int yy = y - o2, xx = x - o1;
+        V[i] = (yy >= 0 && yy < n2 && xx >= 0 && xx < n1) ? src[((long)z * n2 + yy) * n1 + xx] : 0.f;
     }
 }
 
 // lab-frame gradient contribution of a tilt: slab gradient G[s] (n x n,
-// FP64) replicated over the slab's voxels and cropped to the nv^3 volume
-__global__ void k_slab_to_volume(const double *G, float *out, int nv, int n, int b) {
-    const long total = (long)nv * nv * nv;
-    const int o = (n - nv) / 2;
+// FP64) replicated over the slab's voxels and cropped to the [n3][n2][n1] volume
+__global__ void k_slab_to_volume(const double *G, float *out, int n1, int n2, int n3, int n, int b) {
+    const long total = (long)n1 * n2 * n3;
+    const int o1 = (n - n1) / 2, o2 = (n - n2) / 2;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const int z = (int)(i / ((long)nv * nv)), y = (int)((i / nv) % nv), x = (int)(i % nv);
-        out[i] = (float)G[(long)(z / b) * n * n + (long)(y + o) * n + (x + o)];
+        const int z = (int)(i / ((long)n1 * n2)), y = (int)((i / n1) % n2), x = (int)(i % n1);
+        out[i] = (float)G[(long)(z / b) * n * n + (long)(y + o2) * n + (x + o1)];
     }
 }
 
@@ -207,13 +208,13 @@ int vol_positivity(float *v, long n, cudaStream_t st) {
     return (int)cudaGetLastError();
 }
 
-int vol_pad(const float *src, float *V, int nv, int n, cudaStream_t st) {
-    k_pad<<<grid_for((long)n * n * nv), kThreads, 0, st>>>(src, V, nv, n);
+int vol_pad(const float *src, float *V, int n1, int n2, int n3, int n, cudaStream_t st) {
+    k_pad<<<grid_for((long)n * n * n3), kThreads, 0, st>>>(src, V, n1, n2, n3, n);
     return (int)cudaGetLastError();
 }
 
-int vol_slab_to_volume(const double *G, float *out, int nv, int n, int b, cudaStream_t st) {
-    k_slab_to_volume<<<grid_for((long)nv * nv * nv), kThreads, 0, st>>>(G, out, nv, n, b);
+int vol_slab_to_volume(const double *G, float *out, int n1, int n2, int n3, int n, int b, cudaStream_t st) {
+    k_slab_to_volume<<<grid_for((long)n1 * n2 * n3), kThreads, 0, st>>>(G, out, n1, n2, n3, n, b);
     return (int)cudaGetLastError();
 }
 

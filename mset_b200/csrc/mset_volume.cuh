@@ -21,8 +21,9 @@ int vol_max(const float *v, long n, unsigned *bits, float *mx, cudaStream_t st);
 int vol_scale(const float *v, float *out, long n, const float *div, cudaStream_t st);
 int vol_mul(const float *v, float *out, long n, const float *mul, cudaStream_t st);
 int vol_positivity(float *v, long n, cudaStream_t st);
-int vol_pad(const float *src, float *V, int nv, int n, cudaStream_t st);
-int vol_slab_to_volume(const double *G, float *out, int nv, int n, int b, cudaStream_t st);
+// [n3][n2][n1] volume <-> [n3][n][n] window (laterally centred)
+int vol_pad(const float *src, float *V, int n1, int n2, int n3, int n, cudaStream_t st);
+int vol_slab_to_volume(const double *G, float *out, int n1, int n2, int n3, int n, int b, cudaStream_t st);
 int vol_accumulate(const float *g, double *acc, long n, bool zero, cudaStream_t st);
 int vol_update(float *rec, const double *acc, long n, float step0, cudaStream_t st);
 

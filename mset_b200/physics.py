@@ -67,3 +67,59 @@ def normalise_probe(probe: np.ndarray, mean_intensity: float) -> np.ndarray:
     (STEP00_INIT.m:215-218)."""
     s = np.sum(np.abs(np.fft.fft2(probe)) ** 2)
     return probe * np.sqrt(mean_intensity / s)
+
+
+ABERRATIONS = ("C10", "C30", "C50", "C12", "Phi12", "C23", "Phi23", "C21", "Phi21")
+
+
+def check_probe_wave_parameters(ntilts: int, alpha=None, aberration_paras: dict | None = None,
+                                probeDefocus=None) -> dict:
+    """Per-tilt aberration lists as Func_check_probe_wave_parameters.m:20-145
+    makes them: without aberration_paras every coefficient is zero for every
+    tilt; a coefficient given once is broadcast to all tilts, a list must
+    have one entry per tilt (else ValueError, the reference's error), a
+    missing one is zero; a scalar probeDefocus sets C10 = -probeDefocus for
+    every tilt.  Two behaviours of the reference are kept as they are: a
+    per-tilt probeDefocus list is accepted and leaves C10 unchanged (only the
+    scalar case assigns, :136-142), and Phi21 is broadcast when Phi12 (not
+    Phi21) has a single entry (:121); Phi12 is per tilt by then, so for more
+    than one tilt a single Phi21 is an error and Phi21 must be given per tilt.
+    Returns a dict of float64 arrays [ntilts]."""
+    if alpha is None:
+        raise ValueError('input error: put probe forming aperture value (convergence semi-angle) into "alpha".')
+    out = {}
+    if aberration_paras is None:
+        for k in ABERRATIONS:
+            out[k] = np.zeros(ntilts)
+    else:
+        for k in ABERRATIONS:
+            if k not in aberration_paras:
+                out[k] = np.zeros(ntilts)
+                continue
+            v = np.atleast_1d(np.asarray(aberration_paras[k], dtype=np.float64)).ravel()
+            # Phi21 is tested on Phi12's size, as the reference does
+            probe_size = out["Phi12"].size if k == "Phi21" else v.size
+            if probe_size == 1:
+                out[k] = np.ones(ntilts) * v  # broadcast (a per-tilt v passes through elementwise)
+                if out[k].size != ntilts:
+                    raise ValueError(f"input error: make {k} list size and # of tilt angle be same")
+            elif v.size != ntilts:
+                raise ValueError(f"input error: make {k} list size and # of tilt angle be same")
+            else:
+                out[k] = v.copy()
+    if probeDefocus is not None:
+        d = np.atleast_1d(np.asarray(probeDefocus, dtype=np.float64)).ravel()
+        if d.size == 1:
+            out["C10"] = -1.0 * np.ones(ntilts) * d
+        elif d.size != ntilts:
+            raise ValueError("input error: make probeDefocus list size and # of tilt angle be same")
+    return out
+
+
+def probe_waves(n: int, dx: float, lam: float, alpha_mrad: float, paras: dict) -> np.ndarray:
+    """Func_generate_probe_wave.m:14-56 for every tilt of the per-tilt
+    aberration lists `paras` (check_probe_wave_parameters): [ntilts][n][n]
+    complex128, before the per-tilt normalisation of STEP00_INIT.m:215-218"""
+    nt = paras["C10"].size
+    return np.stack([probe_wave(n, dx, lam, alpha_mrad, **{k: float(paras[k][p]) for k in ABERRATIONS})
+                     for p in range(nt)])

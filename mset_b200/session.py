@@ -68,19 +68,26 @@ class Session:
 
     # ---- volume operations of the reconstruction loop ----
     def rotate_volume(self, vol, angles, *, inverse: bool = False, vec1=(0, 0, 1), vec2=(0, 1, 0),
-                      vec3=(1, 0, 0)) -> np.ndarray:
+                      vec3=(1, 0, 0), lines: bool = False) -> np.ndarray:
         """Func_rot_3Dvol_FourierShear / Func_inv_rot_3Dvol_FourierShear of a
-        cubic [n][n][n] volume by (phi, theta, psi) degrees (mset_rotate_volume)"""
+        [n3][n2][n1] volume by (phi, theta, psi) degrees: mset_rotate_volume
+        (plane kernels) for a cubic volume, mset_rotate_volume_nd (line
+        kernels) for any other shape, or for a cubic one with lines=True"""
         v = _c32(vol)
-        n = v.shape[0]
-        if v.shape != (n, n, n):
-            raise ValueError(f"cubic volume expected, got {v.shape}")
+        if v.ndim != 3:
+            raise ValueError(f"3D volume expected, got {v.shape}")
+        n3, n2, n1 = v.shape
         out = np.empty_like(v)
         vecs = [np.ascontiguousarray(np.asarray(x, np.float32)) for x in (vec1, vec2, vec3)]
         a = [float(x) for x in angles]
-        check("mset_rotate_volume", self._lib.mset_rotate_volume(self._h, fptr(v), fptr(out), n, fptr(vecs[0]),
-                                                                 fptr(vecs[1]), fptr(vecs[2]), a[0], a[1], a[2],
-                                                                 int(bool(inverse))))
+        if n1 == n2 == n3 and not lines:
+            check("mset_rotate_volume", self._lib.mset_rotate_volume(self._h, fptr(v), fptr(out), n1, fptr(vecs[0]),
+                                                                     fptr(vecs[1]), fptr(vecs[2]), a[0], a[1], a[2],
+                                                                     int(bool(inverse))))
+        else:
+            check("mset_rotate_volume_nd",
+                  self._lib.mset_rotate_volume_nd(self._h, fptr(v), fptr(out), n1, n2, n3, fptr(vecs[0]),
+                                                  fptr(vecs[1]), fptr(vecs[2]), a[0], a[1], a[2], int(bool(inverse))))
         return out
 
     def tv(self, vol, lam: float, niter: int, fista: bool = False):

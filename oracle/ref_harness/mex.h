@@ -1,10 +1,11 @@
 /*
  * mex.h -- project-written stand-in for MATLAB's MEX API, declaring only the
- * subset the reference's src/CUDA code calls.  Together with mex_shim.cpp it
- * lets the reference's own CUDA path (mex_main.cu, mset.cu, utility.cu,
- * mex_tools.cpp) be compiled unchanged and driven from C.  TEST
- * INFRASTRUCTURE ONLY: the result, oracle/_ref/libmset_ref.so, is a checker
- * and a timed baseline, never part of the product.
+ * subset the reference's src/CUDA code calls (and mxFree).  Together with
+ * mex_shim.cpp it lets the reference's own CUDA path (mex_main.cu, mset.cu,
+ * utility.cu, mex_tools.cpp) be compiled unchanged and driven from C, and
+ * drives this library's MEX gateway (mset_b200/mex/mset_cuda_kernel.cpp) the
+ * same way.  TEST INFRASTRUCTURE ONLY: the results, oracle/_ref/libmset_ref.so
+ * and oracle/_gw/libmset_gateway.so, are checkers and a timed baseline.
  */
 #ifndef MSET_TEST_MEX_SHIM_H
 #define MSET_TEST_MEX_SHIM_H
@@ -52,6 +53,7 @@ mxArray *mxGetFieldByNumber(const mxArray *pm, mwIndex index, int n);
 bool mxIsStruct(const mxArray *pm);
 bool mxIsChar(const mxArray *pm);
 char *mxArrayToString(const mxArray *pm);
+void mxFree(void *ptr);
 #ifdef __cplusplus
 }
 #endif

@@ -149,11 +149,12 @@ mxArray *mxGetFieldByNumber(const mxArray *pm, mwIndex, int n) { return pm->fiel
 bool mxIsStruct(const mxArray *pm) { return pm->cls == mxSTRUCT_CLASS; }
 bool mxIsChar(const mxArray *pm) { return pm->cls == mxCHAR_CLASS; }
 char *mxArrayToString(const mxArray *pm) {
-    // leaked per call, as MATLAB's mxArrayToString leaks when not freed
+    // leaked per call unless the caller mxFree's it, as in MATLAB
     char *s = (char *)std::malloc(pm->str.size() + 1);
     std::memcpy(s, pm->str.c_str(), pm->str.size() + 1);
     return s;
 }
+void mxFree(void *ptr) { std::free(ptr); }
 
 // ---------------------------------------------------------------------------
 // C driver.  Array layouts are the MEX ones: C order [nz][n][n] for RVol
@@ -212,6 +213,12 @@ int ref_run(int mode, float *rvol_out, float *probe_out, float *scan_x_out, floa
     std::memcpy(scan_y_out, plhs[3]->data.data(), plhs[3]->data.size());
     if (err_out) std::memcpy(err_out, plhs[4]->data.data(), 4);
     return 0;
+}
+
+// any mode string with no outputs (the gateways' answer to an unknown mode)
+int ref_mode(const char *mode) {
+    g_outputs.clear();
+    return call(mode, 0, nullptr);
 }
 
 int ref_error(int mode, float *err_out) {

@@ -15,37 +15,45 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libmset_ref.so")
+# this library's MEX gateway (mset_b200/mex/mset_cuda_kernel.cpp) behind the
+# same shim and driver (make -C oracle gw)
+GATEWAY = os.path.join(HERE, "_gw", "libmset_gateway.so")
 _F = C.POINTER(C.c_float)
-_lib = None
+_libs = {}
 
 
-def available() -> bool:
-    return os.path.exists(LIB)
+def available(path: str = LIB) -> bool:
+    return os.path.exists(path)
 
 
-def lib() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        L = C.CDLL(LIB)
+def lib(path: str = LIB) -> C.CDLL:
+    if path not in _libs:
+        L = C.CDLL(path)
         L.ref_last_error.restype = C.c_char_p
         L.ref_upload.argtypes = [C.c_int, C.c_int, _F, _F, _F, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                  _F, _F, _F, C.c_int, _F]
         L.ref_run.argtypes = [C.c_int, _F, _F, _F, _F, _F]
         L.ref_error.argtypes = [C.c_int, _F]
-        _lib = L
-    return _lib
+        L.ref_mode.argtypes = [C.c_char_p]
+        _libs[path] = L
+    return _libs[path]
 
 
 def _f(a):
     return a.ctypes.data_as(_F)
 
 
-def _check(rc):
-    if rc != 0:
-        raise RuntimeError(f"reference MEX call failed ({rc}): {lib().ref_last_error().decode()}")
-
-
 class RefSession:
+    """upload / run / error through a MEX gateway and the shim: the
+    reference's own (default) or this library's (path=GATEWAY)"""
+
+    def __init__(self, path: str = LIB):
+        self.path = path
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(f"MEX call failed ({rc}): {lib(self.path).ref_last_error().decode()}")
+
     def upload(self, rvol, probe, prop, *, sigma, dz, scan_x, scan_y, measured, step=(0, 0, 0), binning=1,
                nsx=None, nsy=None):
         self.rvol = np.ascontiguousarray(rvol, dtype=np.float32)
@@ -59,7 +67,7 @@ class RefSession:
         self.npos = self.sx.size
         nsx = self.npos if nsx is None else nsx
         nsy = 1 if nsy is None else nsy
-        _check(lib().ref_upload(self.n, self.nz, _f(self.rvol), _f(self.probe.view(np.float32)),
+        self._check(lib(self.path).ref_upload(self.n, self.nz, _f(self.rvol), _f(self.probe.view(np.float32)),
                                 _f(self.prop.view(np.float32)), float(sigma), float(dz), int(nsx), int(nsy),
                                 self.npos, _f(self.sx), _f(self.sy), _f(self.step), int(binning), _f(self.meas)))
 
@@ -69,10 +77,10 @@ class RefSession:
         sx = np.empty(self.npos, np.float32)
         sy = np.empty(self.npos, np.float32)
         err = np.zeros(1, np.float32)
-        _check(lib().ref_run(int(mode), _f(rv), _f(pr.view(np.float32)), _f(sx), _f(sy), _f(err)))
+        self._check(lib(self.path).ref_run(int(mode), _f(rv), _f(pr.view(np.float32)), _f(sx), _f(sy), _f(err)))
         return rv, pr, sx, sy, float(err[0])
 
     def error(self, mode=1) -> float:
         err = np.zeros(1, np.float32)
-        _check(lib().ref_error(int(mode), _f(err)))
+        self._check(lib(self.path).ref_error(int(mode), _f(err)))
         return float(err[0])

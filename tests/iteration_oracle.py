@@ -15,17 +15,21 @@ from oracle import tv
 
 
 def pad(v, n):
-    nv = v.shape[0]
-    o = (n - nv) // 2
-    out = np.zeros((nv, n, n), v.dtype)
-    out[:, o:o + nv, o:o + nv] = v
+    """[nv3][nv2][nv1] volume centred laterally in the n x n window"""
+    nv3, nv2, nv1 = v.shape
+    o2, o1 = (n - nv2) // 2, (n - nv1) // 2
+    out = np.zeros((nv3, n, n), v.dtype)
+    out[:, o2:o2 + nv2, o1:o1 + nv1] = v
     return out
 
 
-def crop(g, nv):
+def crop(g, shape):
+    """the [nv3][nv2][nv1] part of a window-sized [*][n][n] array; shape: the
+    volume's shape, or its edge for a cubic one"""
+    nv3, nv2, nv1 = (shape,) * 3 if np.isscalar(shape) else shape
     n = g.shape[1]
-    o = (n - nv) // 2
-    return g[:, o:o + nv, o:o + nv]
+    o2, o1 = (n - nv2) // 2, (n - nv1) // 2
+    return g[:nv3, o2:o2 + nv2, o1:o1 + nv1]
 
 
 def iterate(rec, tilts, prop, angles, *, sigma, dz, binning, step, positivity=True, tv_lambda=0.0, tv_iter=0,
@@ -33,7 +37,7 @@ def iterate(rec, tilts, prop, angles, *, sigma, dz, binning, step, positivity=Tr
     """tilts: list of dicts with probe, sx, sy, meas (updated in place).
     Returns (rec, errs)."""
     nv = rec.shape[0]
-    acc = np.zeros((nv, nv, nv))
+    acc = np.zeros(rec.shape)
     errs = []
     for j, t in enumerate(tilts):
         n = t["probe"].shape[0]
@@ -43,7 +47,7 @@ def iterate(rec, tilts, prop, angles, *, sigma, dz, binning, step, positivity=Tr
         errs.append(e)
         b = nv if method == 2 else binning
         gv = np.repeat(g, b, axis=0)[:nv]
-        acc += O.rot3d(crop(gv, nv), angles[j])
+        acc += O.rot3d(crop(gv, rec.shape), angles[j])
         t["probe"] = (t["probe"] - step[1] * pa).astype(np.complex64)
         t["sx"] = (t["sx"] + step[2] * pd[:, 0]).astype(np.float32)
         t["sy"] = (t["sy"] + step[2] * pd[:, 1]).astype(np.float32)

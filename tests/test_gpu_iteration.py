@@ -44,6 +44,72 @@ def _problem(seed=5):
     return nv, n, b, dz, sigma, prop, angles, tilts, rec0
 
 
+def _problem_nd(seed=7, shape=(24, 24, 32), n=32):
+    """a non-cubic reconstruction [nv3][nv2][nv1] (MATLAB 32 x 24 x 24) in a
+    32^2 window: the rotations of the iteration run as line transforms"""
+    rng = np.random.default_rng(seed)
+    b, dz, E0 = 2, 0.4, 300e3
+    lam = physics.electron_wavelength(E0)
+    sigma = physics.interaction_constant(E0)
+    cz, cy, cx = [int(np.floor((k + 1) / 2 + 0.5)) - 1 for k in shape]
+    z, y, x = np.meshgrid(np.arange(shape[0]) - cz, np.arange(shape[1]) - cy, np.arange(shape[2]) - cx,
+                          indexing="ij")
+    truth = np.zeros(shape)
+    for _ in range(12):
+        p = rng.uniform(-7, 7, 3)
+        truth += rng.uniform(20, 40) * np.exp(-((x - p[0]) ** 2 + (y - p[1]) ** 2 + (z - p[2]) ** 2) / 3.0)
+    angles = [(0, -20, 0), (0, 0, 0), (0, 25, 0)]
+    prop = physics.propagator(n, dz, lam, b)
+    probe = physics.normalise_probe(physics.probe_wave(n, dz, lam, 20.0, C10=-20.0), 1e4).astype(np.complex64)
+    c = np.floor((n + 1) / 2 + 0.5)
+    tilts = []
+    for a in angles:
+        sx = (c + rng.uniform(-5, 5, 4)).astype(np.float32)
+        sy = (c + rng.uniform(-5, 5, 4)).astype(np.float32)
+        Vt = IO.pad(O.rot3d(truth, a, inverse=True), n)
+        meas = np.empty((4, n, n), np.float32)
+        for p in range(4):
+            o = O.position(Vt, probe, prop, sx[p] + 0.3, sy[p] - 0.2, np.zeros((n, n)), sigma=sigma, dz=dz, binning=b)
+            meas[p] = rng.poisson(np.fft.fftshift(np.abs(o["far"]) ** 2))
+        tilts.append(dict(probe=probe.copy(), sx=sx, sy=sy, meas=meas))
+    return shape, n, b, dz, sigma, prop, angles, tilts, (0.6 * truth).astype(np.float32)
+
+
+def test_non_cubic_iteration_matches_oracle(gpu_available):
+    """two iterations (graph) on a 32 x 24 x 24 reconstruction: inverse
+    rotations into the beam frames, the pass, rotations of the gradients back,
+    update, positivity and TV-FISTA, against the FP64 oracle of the same
+    steps (the reference's rotation of unequal sides, oracle.rot3d)"""
+    shape, n, b, dz, sigma, prop, angles, tilts, rec0 = _problem_nd()
+    V0 = IO.pad(O.rot3d(rec0, angles[1], inverse=True), n).astype(np.float32)
+    g, pa, pd, _ = O.batched_tilt(V0, tilts[1]["probe"], prop, tilts[1]["sx"], tilts[1]["sy"], tilts[1]["meas"],
+                                  sigma=sigma, dz=dz, binning=b)
+    step = (0.05 * rec0.max() / np.abs(g).max(), 0.01 * np.abs(tilts[1]["probe"]).max() / np.abs(pa).max(),
+            0.1 / np.abs(pd).max())
+    kw = dict(positivity=True, tv_lambda=0.02, tv_iter=20, tv_fista=True)
+    bs = BatchSession(n=n, nz=shape[0], npos=[4, 4, 4], prop=prop, sigma=sigma, potential_pixelsize=dz,
+                      slice_binning=b, step_size=step)
+    for j, t in enumerate(tilts):
+        bs.set_tilt(j, probe=t["probe"], scan_x=t["sx"], scan_y=t["sy"], measured=t["meas"])
+    bs.iteration_setup(shape, angles, **kw)
+    bs.set_rec(rec0)
+    errs_g, _ = bs.iterate(2)
+    rec_g = bs.get_rec()
+    probes_g = [bs.get_tilt(j)[1] for j in range(3)]
+    bs.close()
+    assert rec_g.shape == shape
+    rec = rec0.astype(np.float64)
+    tl = [dict(t) for t in tilts]
+    errs_o = []
+    for _ in range(2):
+        rec, e = IO.iterate(rec, tl, prop, angles, sigma=sigma, dz=dz, binning=b, step=step, **kw)
+        errs_o.append(e)
+    assert rel_l2(rec_g - rec0, rec - rec0) < 1e-4
+    for j in range(3):
+        assert rel_l2(probes_g[j] - tilts[j]["probe"], tl[j]["probe"] - tilts[j]["probe"]) < 1e-4
+    assert rel_l2(errs_g, np.array(errs_o)) < 1e-4
+
+
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_iteration_matches_oracle(gpu_available, use_graph):
     nv, n, b, dz, sigma, prop, angles, tilts, rec0 = _problem()
@@ -148,3 +214,59 @@ def test_line_search_matches_oracle(gpu_available):
         d_o = np.r_[tl[j]["sx"] - tilts[j]["sx"], tl[j]["sy"] - tilts[j]["sy"]]
         # four accepted iterations of cancellation-limited position sums
         assert rel_l2(d_g, d_o) < 3e-4
+
+
+def test_fifteen_iterations_on_the_small_configuration(gpu_available):
+    """15 iterations of the batched method (one CUDA graph each: rotations,
+    pass, update, positivity, TV-FISTA) on the small configuration's geometry
+    (24^3 volume at 0.4 A in a 64^2 window, 24 slices, 5 tilts over +-30 deg;
+    a 4x4 block of its 12x12 scan per tilt to keep the FP64 oracle within
+    seconds), against the FP64 oracle of the same iteration
+    (Run_MSET_recon.m:111-291 with the batched update).  Stated tolerance for
+    the reconstructed volume after 15 iterations: relative L2 of the change
+    from the start <= 1e-3 (FP32 propagation against FP64, compounded over 15
+    updates; measured 2e-5 - 1e-4), error history <= 1e-4 per iteration."""
+    from mset_b200 import synth
+    cfg = synth.CONFIGS["small"]
+    spec = synth.make_specimen(cfg)
+    n, b = cfg.window, cfg.slice_binning
+    sub = np.array([r * 12 + c for r in range(4, 8) for c in range(4, 8)])  # 4x4 block of the 12x12 raster
+    sx, sy = spec.scan_x[sub], spec.scan_y[sub]
+    tilts = []
+    for j, vt in enumerate(spec.volumes):
+        bs = BatchSession(n=n, nz=vt.shape[0], npos=[sub.size], prop=spec.prop, sigma=spec.sigma,
+                          potential_pixelsize=cfg.dx, slice_binning=b)
+        bs.set_tilt(0, probe=spec.probe, scan_x=sx, scan_y=sy, measured=np.zeros((sub.size, n, n), np.float32),
+                    volume=vt)
+        meas = synth.poisson(bs.simulate(), cfg.seed + 1000 + j)
+        bs.close()
+        tilts.append(dict(probe=spec.probe.copy(), sx=sx.copy(), sy=sy.copy(), meas=meas))
+    angles = [tuple(a) for a in spec.angles]
+    rec0 = (0.5 * spec.lab).astype(np.float32)
+    V0 = IO.pad(O.rot3d(rec0, angles[2], inverse=True), n).astype(np.float32)
+    g, pa, _, _ = O.batched_tilt(V0, spec.probe, spec.prop, sx, sy, tilts[2]["meas"], sigma=spec.sigma, dz=cfg.dx,
+                                 binning=b)
+    step = (0.02 * rec0.max() / np.abs(g).max(), 0.002 * np.abs(spec.probe).max() / np.abs(pa).max(), 0.0)
+    kw = dict(positivity=True, tv_lambda=0.005, tv_iter=30, tv_fista=True)
+    niter = 15
+    bs = BatchSession(n=n, nz=cfg.vol[0], npos=[sub.size] * len(angles), prop=spec.prop, sigma=spec.sigma,
+                      potential_pixelsize=cfg.dx, slice_binning=b, step_size=step)
+    for j, t in enumerate(tilts):
+        bs.set_tilt(j, probe=t["probe"], scan_x=t["sx"], scan_y=t["sy"], measured=t["meas"])
+    bs.iteration_setup(cfg.vol[0], angles, **kw)
+    bs.set_rec(rec0)
+    errs_g, _ = bs.iterate(niter)
+    rec_g = bs.get_rec()
+    bs.close()
+    rec = rec0.astype(np.float64)
+    tl = [dict(t) for t in tilts]
+    errs_o = []
+    for _ in range(niter):
+        rec, e = IO.iterate(rec, tl, spec.prop, angles, sigma=spec.sigma, dz=cfg.dx, binning=b, step=step, **kw)
+        errs_o.append(e)
+    d = rel_l2(rec_g - rec0, rec - rec0)
+    e = [rel_l2(errs_g[i], errs_o[i]) for i in range(niter)]
+    print("15 iterations: volume", f"{d:.2e}", "errors", f"{max(e):.2e}", "error history", errs_g.sum(1)[[0, -1]])
+    assert d < 1e-3
+    assert max(e) < 1e-4
+    assert errs_g.sum(1)[-1] < errs_g.sum(1)[0]  # the iterations reduce the error
