@@ -290,9 +290,9 @@ struct Geo {
 // cluster through distributed shared memory, each task owned by one thread so
 // that the pass is in place.  One distributed pass per column transform, and
 // the switch between row passes and column pass A needs only a CTA barrier.
-template <int N_, int R1_, int NT_, int CL_, int MINB_ = 1>
-struct GeoCl : Geo<N_, R1_, NT_, MINB_> {
-    using Base = Geo<N_, R1_, NT_, MINB_>;
+template <int N_, int R1_, int NT_, int CL_, int MINB_ = 1, bool STAGE_ = false>
+struct GeoCl : Geo<N_, R1_, NT_, MINB_, STAGE_> {
+    using Base = Geo<N_, R1_, NT_, MINB_, STAGE_>;
     static constexpr int CL = CL_;
     static constexpr int ROWS = N_ / CL_;
     static constexpr int N1C = R1_ / CL_;  // residues n1 per CTA

@@ -158,12 +158,17 @@ template <class G>
 struct StageCfg {
     static constexpr int kRows = 32 % G::R1 == 0 ? 32 / G::R1 : 1;  // rows of one warp iteration
     static constexpr int kIters = Own<G>::RPW * G::R1 / 32;          // warp iterations per row pass
-    static constexpr unsigned kBytes = (unsigned)(kRows * G::N * sizeof(float2));
+    static constexpr unsigned kRowBytes = (unsigned)(G::N * sizeof(float2));
+    static constexpr unsigned kBytes = kRows * kRowBytes;
     static constexpr int kWarps = G::NT / 32;
-    static constexpr bool kOn = G::STAGE && G::CL == 1 && 32 % G::R1 == 0 && Own<G>::RPW % kRows == 0 &&
-                                kIters >= 2 && kIters % 2 == 0 && G::R2 <= 8;
-    static constexpr int kStageF2 = kOn ? 2 * kRows * G::N * kWarps : 0;  // stages, float2 units
-    static constexpr int kBarF2 = kOn ? 2 * kWarps : 0;                    // one mbarrier (8 B) per stage
+    // two stages per warp where they fit beside the field and its tables
+    // (227 KB per CTA), else one
+    static constexpr long kBase = (long)sizeof(float2) * (G::FIELD + 6 * G::N) + 4096;
+    static constexpr int kStages = kBase + 2L * kBytes * kWarps <= 227L * 1024 ? 2 : 1;
+    static constexpr bool kOn = G::STAGE && 32 % G::R1 == 0 && Own<G>::RPW % kRows == 0 && kIters >= kStages &&
+                                kIters % kStages == 0 && kBase + (long)kStages * kBytes * kWarps <= 227L * 1024;
+    static constexpr int kStageF2 = kOn ? kStages * kRows * G::N * kWarps : 0;  // stages, float2 units
+    static constexpr int kBarF2 = kOn ? kStages * kWarps : 0;                    // one mbarrier (8 B) per stage
 };
 
 // bounded wait on an mbarrier phase: false if it did not complete within
@@ -187,49 +192,64 @@ template <class G>
 struct RowStage {
     using C = StageCfg<G>;
     static constexpr bool kOn = true;
-    float2 *base;        // this warp's two stages [2][kRows][N]
-    uint32_t bar;        // shared address of this warp's two mbarriers
+    static constexpr int S = C::kStages;
+    float2 *base;        // this warp's stages [S][kRows][N]
+    uint32_t bar;        // shared address of this warp's S mbarriers
     const float2 *src;   // the operand [N][N] in global memory
-    int yl0;             // first row of the warp
-    unsigned phase;      // stage completions before this pass, per stage
+    int yl0;             // first local row of the warp
+    int yb;              // G::ybase() (field rows of a cluster-split CTA)
+    unsigned phase;      // completions of each stage's mbarrier before this pass
     unsigned *fault;     // set when a wait gave up (may be null)
 
-    // request the rows of warp iteration it (lane 0; the stage is free)
+    // request the rows of warp iteration it (lane 0; the stage is free):
+    // one bulk copy of the contiguous rows, or one per row when the field is
+    // split over a cluster (a CTA's consecutive local rows are R1 rows apart)
     __device__ __forceinline__ void issue(int it) const {
-        const float2 *g = src + (size_t)(yl0 + it * C::kRows) * G::N;
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(base + (it & 1) * C::kRows * G::N);
-        const uint32_t b = bar + 8u * (uint32_t)(it & 1);
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(base + (it % S) * C::kRows * G::N);
+        const uint32_t b = bar + 8u * (uint32_t)(it % S);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(C::kBytes) : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                     "l"(g), "r"(C::kBytes), "r"(b)
-                     : "memory");
+        if constexpr (G::CL == 1) {
+            const float2 *g = src + (size_t)(yl0 + it * C::kRows) * G::N;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(dst), "l"(g), "r"(C::kBytes), "r"(b)
+                         : "memory");
+        } else {
+#pragma unroll
+            for (int r = 0; r < C::kRows; ++r) {
+                const float2 *g = src + (size_t)G::gy(yb, yl0 + it * C::kRows + r) * G::N;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        dst + r * C::kRowBytes),
+                    "l"(g), "r"(C::kRowBytes), "r"(b)
+                    : "memory");
+            }
+        }
     }
-    // the first two iterations, at the top of the slab
+    // the first S iterations, at the top of the slab
     __device__ __forceinline__ void start() const {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if ((threadIdx.x & 31) == 0) {
-            issue(0);
-            issue(1);
-        }
+        if ((threadIdx.x & 31) == 0)
+            for (int it = 0; it < S; ++it) issue(it);
     }
     __device__ __forceinline__ void wait(int it) const {
-        const uint32_t b = bar + 8u * (uint32_t)(it & 1);
-        if (!mbar_wait(b, (phase + (unsigned)(it >> 1)) & 1u)) {
+        const uint32_t b = bar + 8u * (uint32_t)(it % S);
+        const unsigned par = (phase + (unsigned)(it / S)) & 1u;
+        if (!mbar_wait(b, par)) {
             if (fault && (threadIdx.x & 31) == 0) atomicOr(fault, 1u);
-            mbar_wait(b, (phase + (unsigned)(it >> 1)) & 1u);  // let a late copy land before reuse
+            mbar_wait(b, par);  // let a late copy land before reuse
         }
     }
-    // every lane has read the stage of iteration it: reuse it for it + 2
+    // every lane has read the stage of iteration it: reuse it for it + S
     __device__ __forceinline__ void refill(int it) const {
-        if (it + 2 >= C::kIters) return;
+        if (it + S >= C::kIters) return;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if ((threadIdx.x & 31) == 0) issue(it + 2);
+        if ((threadIdx.x & 31) == 0) issue(it + S);
     }
     // the task's row in the stage (lane / R1 = row of the iteration, lane % R1 = n1)
     __device__ __forceinline__ const float2 *task(int it, int lane) const {
-        return base + (it & 1) * C::kRows * G::N + (lane / G::R1) * G::N + lane % G::R1;
+        return base + (it % S) * C::kRows * G::N + (lane / G::R1) * G::N + lane % G::R1;
     }
 };
 
@@ -651,9 +671,10 @@ struct PositionKernel {
             using SG = std::conditional_t<kStg, RowStage<G>, NoStage>;
             SG stg{};
             if constexpr (kStg) {
-                stg = RowStage<G>{buf + Smem<G>::STG + 2 * StageCfg<G>::kRows * N * Own<G>::warp(),
-                                  (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 16u * Own<G>::warp(),
-                                  wave, Own<G>::warp() * Own<G>::RPW, stage_phase, a.fault};
+                constexpr int SS = StageCfg<G>::kStages;
+                stg = RowStage<G>{buf + Smem<G>::STG + SS * StageCfg<G>::kRows * N * Own<G>::warp(),
+                                  (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 8u * SS * Own<G>::warp(),
+                                  wave, Own<G>::warp() * Own<G>::RPW, G::ybase(), stage_phase, a.fault};
                 stg.start();
             }
             col_passA<G, +1, false, kColTw<G>>(buf, tw);
@@ -747,7 +768,7 @@ struct PositionKernel {
                         [&](int y, int n1, float2 *v, const APre &pre) { gradop(y, n1, v, pre, nullptr); }, l1);
                 }
             };
-            if constexpr (kStg) stage_phase += StageCfg<G>::kIters / 2;
+            if constexpr (kStg) stage_phase += StageCfg<G>::kIters / StageCfg<G>::kStages;
             if (s > 0) {
                 run_rowA(std::integral_constant<int, -1>{});
                 sync_rows();
@@ -899,9 +920,9 @@ __global__ void __launch_bounds__(G::NT, G::MINB) k_positions(const LaunchArgs a
     if constexpr (StageCfg<G>::kOn) {
         // two mbarriers per warp for the bulk-staged saved-wave rows (one arrival each)
         if ((threadIdx.x & 31) == 0) {
-            const uint32_t b = (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 16u * (threadIdx.x >> 5);
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b + 8u) : "memory");
+            constexpr int SS = StageCfg<G>::kStages;
+            const uint32_t b = (uint32_t)__cvta_generic_to_shared(buf + Smem<G>::BAR) + 8u * SS * (threadIdx.x >> 5);
+            for (int i = 0; i < SS; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b + 8u * i) : "memory");
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -1193,6 +1214,9 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
     }
 // a field split by rows over a cluster of CL_ CTAs
 #define MSET_DEFINE_GEO_CL(N_, R1_, NT_, CL_) MSET_DEFINE_GEO_T(N_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_>))
+// the same with the adjoint's saved-wave rows staged by bulk copies (StageCfg)
+#define MSET_DEFINE_GEO_CL_STAGED(NAME_, N_, R1_, NT_, CL_) \
+    MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_, 1, true>))
 #define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_, MINB_) \
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_, MINB_>))
 #define MSET_UNPAREN(...) __VA_ARGS__
