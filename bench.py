@@ -187,6 +187,8 @@ def run_ours(args):
     if not shard:
         raise SystemExit(f"--gpus {world} exceeds the {ntilts} tilts of the workload")
     cfg, spec, bs, meas, shard = build_problem(args.config, local, shard)
+    if args.variant:
+        bs.set_variant(args.variant)  # another compiled kernel shape of the window (profiling)
     n = cfg.window
     ns = -(-cfg.vol[0] // cfg.slice_binning)
     positions = int(bs.npos.sum())            # this rank's positions
@@ -316,6 +318,7 @@ def run_ours(args):
             "config": {"workload": workload_name(cfg, ns, positions_total),
                        "positions": positions_total, "positions_rank0": positions, "slabs": ns, "window": n,
                        "units_per_step": units_total, "persistent_ctas": bs.shape()["grid"],
+                       "kernel_shape": {k: bs.shape()[k] for k in ("threads", "staged", "checkpoint")},
                        "l2": f"inputs larger than L2 ({meas_bytes / 1e9:.1f} GB measured patterns per GPU)",
                        "parallelism": f"tilts sharded over {world} GPU(s): rank 0 holds tilts "
                                       f"{shard[0]}-{shard[-1]} of {cfg.n_tilts}"},
@@ -665,6 +668,7 @@ def main():
     ap.add_argument("--tv-iter", type=int, default=300, help="TV-FISTA inner iterations per iteration")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-size 6-series group pass")
     ap.add_argument("--no-large", action="store_true", help="skip the 256^2-window (cluster) sample")
+    ap.add_argument("--variant", type=int, default=0, help="kernel shape of the window (0: default; profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
