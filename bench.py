@@ -593,19 +593,23 @@ def host_pass(smp: dict, cores: int):
 def cpu_baseline(args, cfg, spec) -> dict:
     """The single-precision CPU port of the reference's path (oracle/cpu_fp32.c,
     OpenMP over positions, all host threads) on a bounded sample of the same
-    workload (about 10 s of host work on a 16-thread host)."""
+    workload: all 1,024 positions of one tilt, repeated up to about 10 s."""
     from oracle import oracle as O
 
     cores = O.max_threads()
-    smp = host_sample(args.config, min(1024, 32 * cores))
+    smp = host_sample(args.config, 1024)
     k, ns = smp["sx"].size, smp["ns"]
-    t0 = time.perf_counter()
-    host_pass(smp, cores)
+    # passes over the sample until about 10 s of host work (at most 3)
+    reps, t0 = 0, time.perf_counter()
+    while reps < 3 and (reps == 0 or time.perf_counter() - t0 < 10.0):
+        host_pass(smp, cores)
+        reps += 1
     dt = time.perf_counter() - t0
-    return {"value": k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
+    return {"value": reps * k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
             "dtype": "fp32",
-            "sample": f"{k} positions of the 0-degree tilt of the same geometry ({ns} slabs each), single-precision C port "
-                      f"of the reference's CPU path (its MATLAB STEP02/STEP03 run in single), {dt:.1f} s"}
+            "sample": f"{reps} pass(es) over {k} positions of the 0-degree tilt of the same geometry ({ns} slabs "
+                      f"each), single-precision C port of the reference's CPU path (its MATLAB STEP02/STEP03 run "
+                      f"in single), {dt:.1f} s"}
 
 
 def run_reference(args):
