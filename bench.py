@@ -48,9 +48,9 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes per slice-propagation of k_positions at n = 128, 64 slabs:
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
-# kernel on 2 tilts x 64 positions (8192 units): (1.076925 + 1.109599) GB.
+# kernel on 2 tilts x 64 positions (8192 units): (1.076798 + 1.110183) GB.
 # A constant of this bench (ncu does not run inside it), scaled by units.
-TRAFFIC_PER_UNIT = (1.076925e9 + 1.109599e9) / 8192
+TRAFFIC_PER_UNIT = (1.076798e9 + 1.110183e9) / 8192
 
 
 def flops_per_unit(n: int) -> float:

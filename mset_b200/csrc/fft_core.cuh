@@ -217,7 +217,7 @@ struct Split {
 };
 template <int R, int SG>
 struct DFT {
-    static_assert(R == 6 || R == 8 || R == 10 || R == 12 || R == 16 || R == 9 || R == 15 || R == 20,
+    static_assert(R == 6 || R == 8 || R == 10 || R == 12 || R == 16 || R == 9 || R == 15 || R == 20 || R == 32,
                   "unsupported codelet size");
     static __device__ __forceinline__ void run(float2 *v) {
         constexpr int P = Split<R>::P, Q = Split<R>::Q;
@@ -268,11 +268,16 @@ struct Geo {
     static constexpr int CL = 1;          // CTAs sharing one field (thread-block cluster)
     static constexpr int ROWS = N;        // rows of the field held by one CTA
     static constexpr int FIELD = ROWS * S;
+    static constexpr bool THREE = false;  // the three-phase shape (Geo3)
+    static constexpr int CB = R1;         // points of a column-pass-B task
+    static constexpr int RY1 = R1;        // the y dimension's factors (the x ones here)
     static_assert(R1 * R2 == N, "N must equal R1*R2");
     __device__ __forceinline__ static int px(int x) { return x + x / R1; }
     __device__ __forceinline__ static int at(int y, int x) { return y * S + px(x); }
-    // scrambled location -> frequency index
+    // scrambled location -> frequency index (both dimensions)
     __host__ __device__ __forceinline__ static int scr(int L) { return L / R1 + R2 * (L % R1); }
+    __host__ __device__ __forceinline__ static int scrx(int L) { return scr(L); }
+    __host__ __device__ __forceinline__ static int scry(int L) { return scr(L); }
     __device__ __forceinline__ static int rank() { return 0; }
     // row of the field held at local row l (yb = ybase(), read once per pass)
     __device__ __forceinline__ static int ybase() { return 0; }
@@ -306,6 +311,56 @@ struct GeoCl : Geo<N_, R1_, NT_, MINB_, STAGE_> {
     }
     __device__ __forceinline__ static int ybase() { return rank() * N1C; }
     __device__ __forceinline__ static int gy(int yb, int l) { return yb + l / Base::R2 + R1_ * (l % Base::R2); }
+};
+
+// Three-phase shape of a 128 x 128 field (one CTA of 512 threads).  The
+// two-pass shape above costs six shared-memory round trips per propagation
+// slab.  Here a 2D transform is three register phases of 16 or 32 points:
+//
+//   phase 1 (rows)  task (y, n1):  x = n1 + 8 j, j < 16        DFT16 over j
+//   phase 2         task (k1, b):  x = a + 8 k1, a < 8         twiddle W^(a k1), DFT8 over a
+//                                  y = b + 32 m, m < 4         DFT4 over m, twiddle W^(b k1')
+//   phase 3 (cols)  task (x, k1'): y = b + 32 k1', b < 32      DFT32 over b
+//
+// (natural -> scrambled; the way back runs the phases in reverse with the
+// twiddles on the other side of each DFT).  Location Lx = k2 + 8 k1 then
+// holds frequency k1 + 16 k2 and Ly = k2' + 32 k1' frequency k1' + 4 k2'.
+// The phases bordering a pointwise stage are fused as in the two-pass shape
+// (phase 1 = inverse rows + op + forward rows, phase 3 = forward columns + op
+// + inverse columns), so a slab costs four round trips.  Warp w's phase-1
+// rows {2w, 2w+1} + 32 m are the rows of its phase-2 tasks: phases 1 and 2
+// meet at a warp barrier, phases 2 and 3 at a CTA barrier.  Rows are padded
+// after every 8 elements and to a stride of 8 mod 16 elements, under which
+// the accesses of all three phases are free of bank conflicts with constant
+// offsets from one base address per task.  WIDE: two pad elements per 8 (row
+// stride 168), so that phase 2 moves its 8 consecutive x values as four
+// 16-byte accesses (half the shared-memory instructions of that phase); one
+// pad element per 8 (stride 152) otherwise.
+template <int MINB_ = 1, bool WIDE_ = false>
+struct Geo3 {
+    static constexpr bool THREE = true;
+    static constexpr bool WIDE = WIDE_;
+    static constexpr int MINB = MINB_;
+    static constexpr bool STAGE = false;
+    static constexpr int N = 128;
+    static constexpr int R1 = 8, R2 = 16;   // x: phase-1 task (y, n1) holds x = n1 + R1 j, j < R2
+    static constexpr int RY1 = 32, RY2 = 4;  // y: phase 2 radix RY2 at stride RY1, phase 3 radix RY1
+    static constexpr int CB = RY1;           // points of a column (phase-3) task
+    static constexpr int NT = 512;
+    static constexpr int PADX = WIDE_ ? 2 : 1;   // pad elements after every R1
+    static constexpr int GS = R1 + PADX;         // stride of x = n1 + R1 j over j
+    static constexpr int S = N + PADX * (N / R1) + 8;  // 152 or 168
+    static constexpr int CL = 1;
+    static constexpr int ROWS = N;
+    static constexpr int FIELD = ROWS * S;
+    static_assert(S % 16 == 8, "rows 2w and 2w+1 must fall on opposite bank halves");
+    __device__ __forceinline__ static int px(int x) { return x + PADX * (x / R1); }
+    __device__ __forceinline__ static int at(int y, int x) { return y * S + px(x); }
+    __host__ __device__ __forceinline__ static int scrx(int L) { return L / R1 + R2 * (L % R1); }
+    __host__ __device__ __forceinline__ static int scry(int L) { return L / RY1 + RY2 * (L % RY1); }
+    __device__ __forceinline__ static int rank() { return 0; }
+    __device__ __forceinline__ static int ybase() { return 0; }
+    __device__ __forceinline__ static int gy(int, int l) { return l; }
 };
 
 // twiddle W_N^{n1 k2} with sign (table holds e^{-2 pi i m/N} as [k2][n1])
@@ -346,6 +401,9 @@ __device__ __forceinline__ void sync_cols() {
     if constexpr (G::CL > 1) {
         // column pass B touches rows of other CTAs
         cluster_sync();
+    } else if constexpr (G::THREE) {
+        // phase 2 and phase 3 tasks share no rows or columns
+        __syncthreads();
     } else {
         // named barrier per warp pair (ids 1..15; 0 is __syncthreads)
         asm volatile("bar.sync %0, 64;" ::"r"(1 + Own<G>::pair()) : "memory");
@@ -406,78 +464,118 @@ struct NoStage {
     __device__ __forceinline__ const float2 *task(int, int) const { return nullptr; }
 };
 
-template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1 = NoL1, class ST = NoStage>
-__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op, L1 &&l1 = NoL1{},
-                                             const ST &st = ST{}) {
-    using O = Own<G>;
+// Phase 1 of the three-phase shape (Geo3): row pass A without twiddles (they
+// belong to phase 2).  Lane l of warp w takes n1 = l % 8 and the rows
+// 2w + (l / 8) % 2 + 32 (l / 16) and 64 below it; the callbacks are row pass
+// A's.
+template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1, class ST>
+__device__ __forceinline__ void rows3(float2 *buf, Pf &&pf, Op &&op, const L1 &, const ST &) {
+    static_assert(!ST::kOn && std::decay_t<L1>::kLines == 0, "no staged operands or L1 hints in phase 1");
     constexpr int R1 = G::R1, R2 = G::R2;
-    constexpr int TASKS = O::RPW * R1;
-    static_assert(!ST::kOn || TASKS % 32 == 0, "a staged operand needs whole warp iterations");
-    const int yl0 = O::warp() * O::RPW;  // first local row of the warp
-    const int yb = G::ybase();           // local row -> row of the field (pf / op)
-    // Pre::kAhead: issue the next task's global loads while the current task
-    // runs (double-buffered prefetch); otherwise just before its shared reads
+    const int lane = threadIdx.x & 31;
+    const int n1 = lane % R1;
+    const int y0 = 2 * (threadIdx.x >> 5) + ((lane >> 3) & 1) + 32 * (lane >> 4);
     constexpr bool ahead = Pre::kAhead;
     Pre pre, nxt;
-    if (ahead && O::lane() < TASKS) pf(G::gy(yb, yl0 + O::lane() / R1), O::lane() % R1, pre);
-    // a lane's residue n1 is the same in every task when R1 divides 32, so
-    // its twiddles W^(n1 k2) stay in registers for the whole pass instead of
-    // being read from shared memory twice per task (while R2 <= 8 leaves
-    // room for them)
-    constexpr bool kTwReg = (32 % R1 == 0) && R2 <= 8 && (IN != 0 || OUT != 0);
-    float2 twr[kTwReg ? R2 : 1];
-    if constexpr (kTwReg) {
-#pragma unroll
-        for (int k2 = 1; k2 < R2; ++k2) twr[k2] = tw[k2 * R1 + O::lane() % R1];
-    }
+    if constexpr (ahead) pf(y0, n1, pre);
 #pragma unroll 1
-    for (int tau = O::lane(); tau < TASKS; tau += 32) {
-        const int n1 = tau % R1, y = G::gy(yb, yl0 + tau / R1);
-        if constexpr (std::decay_t<L1>::kLines > 0) {
-            // pull the next iteration's rows of the op's global operands into
-            // L1 (hints: no registers, no scoreboard)
-            constexpr int LN = std::decay_t<L1>::kLines, RI = 32 / R1;
-            const int r0 = yl0 + (tau - O::lane() + 32) / R1;
-            if (r0 < yl0 + O::RPW)
-                for (int q = O::lane(); q < RI * LN; q += 32) l1(G::gy(yb, r0 + q / LN), q % LN);
-        }
+    for (int it = 0; it < 2; ++it) {
+        const int y = y0 + 64 * it;
         if constexpr (ahead) {
-            if (tau + 32 < TASKS) pf(G::gy(yb, yl0 + (tau + 32) / R1), (tau + 32) % R1, nxt);
+            if (it == 0) pf(y0 + 64, n1, nxt);
         } else {
             pf(y, n1, pre);
         }
-        float2 *row = buf + (yl0 + tau / R1) * G::S + n1;
+        float2 *row = buf + y * G::S + n1;
         float2 v[R2];
 #pragma unroll
-        for (int j = 0; j < R2; ++j) v[j] = row[(R1 + 1) * j];
-        auto twi = [&](int k2, auto sg) -> float2 {
-            constexpr int SG = decltype(sg)::value;
-            if constexpr (kTwReg) return SG < 0 ? twr[k2] : cconj(twr[k2]);
-            else return twN<G, SG>(tw, n1, k2);
-        };
-        if constexpr (IN != 0) {
+        for (int j = 0; j < R2; ++j) v[j] = row[G::GS * j];
+        if constexpr (IN != 0) DFT<R2, IN>::run(v);
+        op(y, n1, v, pre);
+        if constexpr (OUT != 0) DFT<R2, OUT>::run(v);
 #pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, IN>{}));
-            DFT<R2, IN>::run(v);
-        }
-        if constexpr (ST::kOn) {
-            // the staged operand rows of this warp iteration: wait for their
-            // bulk copy, hand the task its row, refill the stage afterwards
-            const int it = (tau - O::lane()) >> 5;
-            st.wait(it);
-            op(y, n1, v, pre, st.task(it, O::lane()));
-            st.refill(it);
-        } else {
-            op(y, n1, v, pre);
-        }
-        if constexpr (OUT != 0) {
-            DFT<R2, OUT>::run(v);
-#pragma unroll
-            for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, OUT>{}));
-        }
-#pragma unroll
-        for (int j = 0; j < R2; ++j) row[(R1 + 1) * j] = v[j];
+        for (int j = 0; j < R2; ++j) row[G::GS * j] = v[j];
         if constexpr (ahead) pre = nxt;
+    }
+}
+
+template <class G, int IN, int OUT, class Pre, class Pf, class Op, class L1 = NoL1, class ST = NoStage>
+__device__ __forceinline__ void row_passA_pf(float2 *buf, const float2 *tw, Pf &&pf, Op &&op, L1 &&l1 = NoL1{},
+                                             const ST &st = ST{}) {
+    if constexpr (G::THREE) {
+        rows3<G, IN, OUT, Pre>(buf, pf, op, l1, st);
+        (void)tw;
+    } else {
+        using O = Own<G>;
+        constexpr int R1 = G::R1, R2 = G::R2;
+        constexpr int TASKS = O::RPW * R1;
+        static_assert(!ST::kOn || TASKS % 32 == 0, "a staged operand needs whole warp iterations");
+        const int yl0 = O::warp() * O::RPW;  // first local row of the warp
+        const int yb = G::ybase();           // local row -> row of the field (pf / op)
+        // Pre::kAhead: issue the next task's global loads while the current task
+        // runs (double-buffered prefetch); otherwise just before its shared reads
+        constexpr bool ahead = Pre::kAhead;
+        Pre pre, nxt;
+        if (ahead && O::lane() < TASKS) pf(G::gy(yb, yl0 + O::lane() / R1), O::lane() % R1, pre);
+        // a lane's residue n1 is the same in every task when R1 divides 32, so
+        // its twiddles W^(n1 k2) stay in registers for the whole pass instead of
+        // being read from shared memory twice per task (while R2 <= 8 leaves
+        // room for them)
+        constexpr bool kTwReg = (32 % R1 == 0) && R2 <= 8 && (IN != 0 || OUT != 0);
+        float2 twr[kTwReg ? R2 : 1];
+        if constexpr (kTwReg) {
+#pragma unroll
+            for (int k2 = 1; k2 < R2; ++k2) twr[k2] = tw[k2 * R1 + O::lane() % R1];
+        }
+#pragma unroll 1
+        for (int tau = O::lane(); tau < TASKS; tau += 32) {
+            const int n1 = tau % R1, y = G::gy(yb, yl0 + tau / R1);
+            if constexpr (std::decay_t<L1>::kLines > 0) {
+                // pull the next iteration's rows of the op's global operands into
+                // L1 (hints: no registers, no scoreboard)
+                constexpr int LN = std::decay_t<L1>::kLines, RI = 32 / R1;
+                const int r0 = yl0 + (tau - O::lane() + 32) / R1;
+                if (r0 < yl0 + O::RPW)
+                    for (int q = O::lane(); q < RI * LN; q += 32) l1(G::gy(yb, r0 + q / LN), q % LN);
+            }
+            if constexpr (ahead) {
+                if (tau + 32 < TASKS) pf(G::gy(yb, yl0 + (tau + 32) / R1), (tau + 32) % R1, nxt);
+            } else {
+                pf(y, n1, pre);
+            }
+            float2 *row = buf + (yl0 + tau / R1) * G::S + n1;
+            float2 v[R2];
+#pragma unroll
+            for (int j = 0; j < R2; ++j) v[j] = row[(R1 + 1) * j];
+            auto twi = [&](int k2, auto sg) -> float2 {
+                constexpr int SG = decltype(sg)::value;
+                if constexpr (kTwReg) return SG < 0 ? twr[k2] : cconj(twr[k2]);
+                else return twN<G, SG>(tw, n1, k2);
+            };
+            if constexpr (IN != 0) {
+#pragma unroll
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, IN>{}));
+                DFT<R2, IN>::run(v);
+            }
+            if constexpr (ST::kOn) {
+                // the staged operand rows of this warp iteration: wait for their
+                // bulk copy, hand the task its row, refill the stage afterwards
+                const int it = (tau - O::lane()) >> 5;
+                st.wait(it);
+                op(y, n1, v, pre, st.task(it, O::lane()));
+                st.refill(it);
+            } else {
+                op(y, n1, v, pre);
+            }
+            if constexpr (OUT != 0) {
+                DFT<R2, OUT>::run(v);
+#pragma unroll
+                for (int k2 = 1; k2 < R2; ++k2) v[k2] = cmul(v[k2], twi(k2, std::integral_constant<int, OUT>{}));
+            }
+#pragma unroll
+            for (int j = 0; j < R2; ++j) row[(R1 + 1) * j] = v[j];
+            if constexpr (ahead) pre = nxt;
+        }
     }
 }
 
@@ -613,7 +711,28 @@ template <class G, int IN, int OUT, class Op>
 __device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
     using O = Own<G>;
     constexpr int R1 = G::R1, R2 = G::R2;
-    if constexpr (G::CL > 1) {
+    if constexpr (G::THREE) {
+        // phase 3: half-warp h of warp w takes the pair q = 2w + h, rows
+        // 32 (q / 8) + b and the column groups c and c + D (columns 8 c + i,
+        // i < 8) that fall on opposite bank halves: D = 8 with one pad
+        // element per 8 columns (9 D = 8 mod 16), D = 4 with two (10 D = 8)
+        const int lane = threadIdx.x & 31;
+        const int q = 2 * (threadIdx.x >> 5) + (lane >> 4), g = q & 7;
+        constexpr int D = G::PADX == 1 ? 8 : 4;
+        static_assert((G::GS * D) % 16 == 8, "the two column groups of a half-warp share no bank");
+        const int c = D == 8 ? g : (g & 3) + 8 * (g >> 2);
+        const int x = 8 * c + (lane & 7) + 8 * D * ((lane >> 3) & 1);
+        const int y0 = G::RY1 * (q >> 3);
+        float2 *p = buf + y0 * G::S + G::px(x);
+        float2 v[G::CB];
+#pragma unroll
+        for (int j = 0; j < G::CB; ++j) v[j] = p[G::S * j];
+        if constexpr (IN != 0) DFT<G::CB, IN>::run(v);
+        op(y0, x, v);
+        if constexpr (OUT != 0) DFT<G::CB, OUT>::run(v);
+#pragma unroll
+        for (int j = 0; j < G::CB; ++j) p[G::S * j] = v[j];
+    } else if constexpr (G::CL > 1) {
         // distributed: CTA r owns the tasks k2 in [r*K2C, (r+1)*K2C) of every
         // column; element j (row j + R1*k2, residue j) lives in CTA j / N1C at
         // local row (j % N1C)*R2 + k2
@@ -638,23 +757,135 @@ __device__ __forceinline__ void col_passB(float2 *buf, Op &&op) {
 #pragma unroll
             for (int j = 0; j < R1; ++j) st_cluster(pb[j / G::N1C] + off + kRes * (j % G::N1C), v[j]);
         }
-        return;
-    }
-    constexpr int TASKS = O::CPP * R2;
-    const int x0 = O::pair() * O::CPP;
+    } else {
+        constexpr int TASKS = O::CPP * R2;
+        const int x0 = O::pair() * O::CPP;
 #pragma unroll 1
-    for (int tau = O::plane(); tau < TASKS; tau += 64) {
-        const int x = x0 + tau % O::CPP, k2 = tau / O::CPP;
-        const int y0 = R1 * k2;
-        float2 *p = buf + y0 * G::S + G::px(x);
-        float2 v[R1];
+        for (int tau = O::plane(); tau < TASKS; tau += 64) {
+            const int x = x0 + tau % O::CPP, k2 = tau / O::CPP;
+            const int y0 = R1 * k2;
+            float2 *p = buf + y0 * G::S + G::px(x);
+            float2 v[R1];
 #pragma unroll
-        for (int j = 0; j < R1; ++j) v[j] = p[G::S * j];
-        if constexpr (IN != 0) DFT<R1, IN>::run(v);
-        op(y0, x, v);
-        if constexpr (OUT != 0) DFT<R1, OUT>::run(v);
+            for (int j = 0; j < R1; ++j) v[j] = p[G::S * j];
+            if constexpr (IN != 0) DFT<R1, IN>::run(v);
+            op(y0, x, v);
+            if constexpr (OUT != 0) DFT<R1, OUT>::run(v);
 #pragma unroll
-        for (int j = 0; j < R1; ++j) p[G::S * j] = v[j];
+            for (int j = 0; j < R1; ++j) p[G::S * j] = v[j];
+        }
+    }
+}
+
+// Phase 2 of the three-phase shape: lane l of warp w takes k1 = l % 16 and
+// b = 2w + l / 16, element (a, m) at x = a + 8 k1, y = b + 32 m.  FWD: the
+// natural -> scrambled step; else scrambled -> natural.  The twiddle tables
+// are tw[16 a + k1] = W^(a k1) and tw[N + 32 k1' + b] = W^(b k1') (sign -1).
+template <class G, int SG, bool FWD>
+__device__ __forceinline__ void mid3(float2 *buf, const float2 *tw) {
+    constexpr int RX = G::R1, RY = G::RY2, KX = G::R2;  // 8-point x DFTs, 4-point y DFTs, 16 k1
+    const int lane = threadIdx.x & 31;
+    const int k1 = lane % KX, b = 2 * (threadIdx.x >> 5) + lane / KX;
+    float2 *p = buf + b * G::S + G::GS * k1;
+    float2 v[RX * RY];  // v[a + 8 m]
+    if constexpr (G::WIDE) {
+        // 16-byte pairs (p is 16-byte aligned: S and GS are even)
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+#pragma unroll
+            for (int a = 0; a < RX; a += 2) {
+                const float4 t = *reinterpret_cast<const float4 *>(p + G::RY1 * G::S * m + a);
+                v[a + RX * m] = make_float2(t.x, t.y);
+                v[a + 1 + RX * m] = make_float2(t.z, t.w);
+            }
+    } else {
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+#pragma unroll
+            for (int a = 0; a < RX; ++a) v[a + RX * m] = p[G::RY1 * G::S * m + a];
+    }
+    const float2 *twx = tw + k1;
+    const float2 *twy = tw + G::N + b;
+    auto wx = [&](int a) { const float2 t = twx[KX * a]; return SG < 0 ? t : cconj(t); };
+    auto wy = [&](int k) { const float2 t = twy[G::RY1 * k]; return SG < 0 ? t : cconj(t); };
+    auto xdft = [&]() {
+#pragma unroll
+        for (int m = 0; m < RY; ++m) DFT<RX, SG>::run(v + RX * m);
+    };
+    auto ydft = [&]() {
+#pragma unroll
+        for (int a = 0; a < RX; ++a) {
+            float2 u[RY];
+#pragma unroll
+            for (int m = 0; m < RY; ++m) u[m] = v[a + RX * m];
+            DFT<RY, SG>::run(u);
+#pragma unroll
+            for (int m = 0; m < RY; ++m) v[a + RX * m] = u[m];
+        }
+    };
+    auto xtw = [&]() {
+#pragma unroll
+        for (int a = 1; a < RX; ++a) {
+            const float2 t = wx(a);
+#pragma unroll
+            for (int m = 0; m < RY; ++m) v[a + RX * m] = cmul(v[a + RX * m], t);
+        }
+    };
+    auto ytw = [&]() {
+#pragma unroll
+        for (int k = 1; k < RY; ++k) {
+            const float2 t = wy(k);
+#pragma unroll
+            for (int a = 0; a < RX; ++a) v[a + RX * k] = cmul(v[a + RX * k], t);
+        }
+    };
+    if constexpr (FWD) {
+        xtw();
+        xdft();
+        ydft();
+        ytw();
+    } else {
+        ytw();
+        ydft();
+        xdft();
+        xtw();
+    }
+    if constexpr (G::WIDE) {
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+#pragma unroll
+            for (int a = 0; a < RX; a += 2)
+                *reinterpret_cast<float4 *>(p + G::RY1 * G::S * m + a) =
+                    make_float4(v[a + RX * m].x, v[a + RX * m].y, v[a + 1 + RX * m].x, v[a + 1 + RX * m].y);
+    } else {
+#pragma unroll
+        for (int m = 0; m < RY; ++m)
+#pragma unroll
+            for (int a = 0; a < RX; ++a) p[G::RY1 * G::S * m + a] = v[a + RX * m];
+    }
+}
+
+// The steps between the row-side pass A and column pass B of a transform:
+// natural -> scrambled (mid_fwd: row pass B, column pass A) and back
+// (mid_inv), sign SG.  TT: column pass A reads the transposed twiddle table.
+template <class G, int SG, bool TT>
+__device__ __forceinline__ void mid_fwd(float2 *buf, const float2 *tw) {
+    if constexpr (G::THREE) {
+        mid3<G, SG, true>(buf, tw);
+    } else {
+        row_passB<G, SG>(buf);
+        sync_rowcol();
+        col_passA<G, SG, true, TT>(buf, tw);
+    }
+}
+template <class G, int SG, bool TT>
+__device__ __forceinline__ void mid_inv(float2 *buf, const float2 *tw) {
+    if constexpr (G::THREE) {
+        mid3<G, SG, false>(buf, tw);
+    } else {
+        col_passA<G, SG, false, TT>(buf, tw);
+        sync_rowcol();
+        row_passB<G, SG>(buf);
     }
 }
 

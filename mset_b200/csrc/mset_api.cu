@@ -176,31 +176,59 @@ int set_device(mset_session *s) {
     return 0;
 }
 
-// twiddle table e^{-2 pi i n1 k2 / N} stored as [k2][n1], computed in double
+// e^{-2 pi i m / n} in double, rounded to float
+float2 twiddle(long m, int n) {
+    const double a = -2.0 * M_PI * (double)(m % n) / (double)n;
+    return make_float2((float)std::cos(a), (float)std::sin(a));
+}
+
+// twiddle tables of the plan's shape: e^{-2 pi i n1 k2 / N} as [k2][n1]
+// (two-pass shape), or the three-phase shape's x table [a][k1] (a < r1) and
+// y table [k1'][b] (b < ry1) one after the other
 int upload_twiddles(mset_session *s) {
     const int n = s->plan.n, r1 = s->plan.r1, r2 = n / r1;
-    std::vector<float2> h(n);
-    for (int k2 = 0; k2 < r2; ++k2)
-        for (int n1 = 0; n1 < r1; ++n1) {
-            const long m = (long)n1 * k2 % n;
-            const double a = -2.0 * M_PI * (double)m / (double)n;
-            h[k2 * r1 + n1] = make_float2((float)std::cos(a), (float)std::sin(a));
-        }
-    CK(s->twn.ensure(n));
-    CK(cudaMemcpyAsync(s->twn.p, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, s->st));
+    const bool three = s->plan.ry1 != s->plan.r1;
+    std::vector<float2> h(three ? 2 * n : n);
+    if (three) {
+        const int ry1 = s->plan.ry1, ry2 = n / ry1;
+        for (int a = 0; a < r1; ++a)
+            for (int k1 = 0; k1 < r2; ++k1) h[a * r2 + k1] = twiddle((long)a * k1, n);
+        for (int k = 0; k < ry2; ++k)
+            for (int b = 0; b < ry1; ++b) h[n + k * ry1 + b] = twiddle((long)b * k, n);
+    } else {
+        for (int k2 = 0; k2 < r2; ++k2)
+            for (int n1 = 0; n1 < r1; ++n1) h[k2 * r1 + n1] = twiddle((long)n1 * k2, n);
+    }
+    CK(s->twn.ensure(h.size()));
+    CK(cudaMemcpyAsync(s->twn.p, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, s->st));
     return 0;
 }
 
-int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz, const float *prop) {
+// frequency index held at scrambled location L of a dimension with r residues
+int scrambled_freq(int L, int n, int r) { return L / r + (n / r) * (L % r); }
+
+// sequential: the session serves the sequential entry points (upload / run /
+// per-position steps), whose one-CTA shape takes the scrambled layouts of the
+// window's cluster geometry for that pass when one is compiled
+int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz, const float *prop,
+                    bool sequential) {
     if (n <= 1 || nz <= 0 || b <= 0) return fail(MSET_E_ARG, "invalid sizes n=%d nz=%d slice_binning=%d", n, nz, b);
     Plan pl;
     if (!plan_for(n, &pl))
         return fail(MSET_E_UNSUPPORTED,
                     "window size %d has no compiled kernel (supported: 24, 32, 48, 64, 96, 128, 160, 256)", n);
     if (b > nz) b = nz;  // STEP00_INIT.m:126-128
+    Plan sq{};
+    bool has_seq = plan_seq_for(n, &sq);
+    if (sequential && has_seq && (sq.r1 != pl.r1 || sq.ry1 != pl.ry1)) {
+        Plan alt;
+        if (plan_for_layout(n, sq.r1, sq.ry1, &alt)) pl = alt;
+    }
+    has_seq = has_seq && sq.r1 == pl.r1 && sq.ry1 == pl.ry1;
     if (pl.cl > 1) pl.max_clusters = pl.ops->max_clusters();
     s->plan = pl;
-    s->has_seq = plan_seq_for(n, &s->seq_plan);
+    s->seq_plan = sq;
+    s->has_seq = has_seq;
     s->n = n;
     s->nz = nz;
     s->b = b;
@@ -220,7 +248,7 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
     // is separable to FP32 rounding, the kernels keep the two vectors in
     // shared memory instead of reading the n x n table.
     {
-        const int h = (n + 1) / 2, r1 = pl.r1, r2 = n / r1;
+        const int h = (n + 1) / 2;
         std::vector<double> re(n2), im(n2);
         double mx = 0;
         for (int r = 0; r < n; ++r)
@@ -245,9 +273,9 @@ int ensure_geometry(mset_session *s, int n, int nz, int b, float sigma, float dz
         if (s->sep) {
             std::vector<float2> h2(2 * n);
             for (int L = 0; L < n; ++L) {
-                const int k = L / r1 + r2 * (L % r1);
-                h2[L] = make_float2((float)(re[(size_t)k * n] / n), (float)(im[(size_t)k * n] / n));
-                const double vr = (re[k] * a0 + im[k] * b0) / d0, vi = (im[k] * a0 - re[k] * b0) / d0;
+                const int ky = scrambled_freq(L, n, pl.ry1), kx = scrambled_freq(L, n, pl.r1);
+                h2[L] = make_float2((float)(re[(size_t)ky * n] / n), (float)(im[(size_t)ky * n] / n));
+                const double vr = (re[kx] * a0 + im[kx] * b0) / d0, vi = (im[kx] * a0 - re[kx] * b0) / d0;
                 h2[n + L] = make_float2((float)(vr / n), (float)(vi / n));
             }
             CK(s->psep.ensure(2 * n));
@@ -506,7 +534,7 @@ static int upload_impl(mset_session *s, const mset_upload_args *a, const float *
     s->batch = false;
     s->step_k = -1;
     s->ckpt = 0;  // the sequential kernels keep every slab's wave
-    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
+    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D, true);
     if (rc) return rc;
     s->step[0] = a->step_size[0];
     s->step[1] = a->step_size[1];
@@ -617,8 +645,8 @@ int mset_error(mset_session *s, int mode, float *error_out) {
 
 // centred (MATLAB fftshift) index of scrambled location L: frequency scr(L)
 // moved by floor(n/2)
-static int centred_of_scrambled(int L, int n, int r1) {
-    const int k = L / r1 + (n / r1) * (L % r1);
+static int centred_of_scrambled(int L, int n, int r) {
+    const int k = scrambled_freq(L, n, r);
     int c = k - (n + 1) / 2;
     return c < 0 ? c + n : c;
 }
@@ -673,7 +701,7 @@ int mset_forward_position(mset_session *s, int mode, int k, float row, float col
     if (resi_out) {
         float2 *ro = reinterpret_cast<float2 *>(resi_out);
         for (int Ly = 0; Ly < n; ++Ly) {
-            const int r = centred_of_scrambled(Ly, n, s->plan.r1);
+            const int r = centred_of_scrambled(Ly, n, s->plan.ry1);
             for (int Lx = 0; Lx < n; ++Lx)
                 ro[(size_t)r * n + centred_of_scrambled(Lx, n, s->plan.r1)] = resi[(size_t)Ly * n + Lx];
         }
@@ -706,7 +734,7 @@ int mset_adjoint_position(mset_session *s, int mode, int adjoint, const float *r
         const float2 *ri = reinterpret_cast<const float2 *>(resi_in);
         std::vector<float2> scr(n2);
         for (int Ly = 0; Ly < n; ++Ly) {
-            const int r = centred_of_scrambled(Ly, n, s->plan.r1);
+            const int r = centred_of_scrambled(Ly, n, s->plan.ry1);
             for (int Lx = 0; Lx < n; ++Lx)
                 scr[(size_t)Ly * n + Lx] = ri[(size_t)r * n + centred_of_scrambled(Lx, n, s->plan.r1)];
         }
@@ -817,7 +845,7 @@ int mset_batch_setup(mset_session *s, const mset_batch_args *a) {
     int rc = set_device(s);
     if (rc) return rc;
     s->ready = false;
-    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D);
+    rc = ensure_geometry(s, a->n, a->nz, a->slice_binning, a->sigma, a->potential_pixelsize, a->prop2D, false);
     if (rc) return rc;
     s->method = a->method;
     s->adjoint = a->adjoint;
@@ -1014,11 +1042,11 @@ int mset_batch_read_gradient(mset_session *s, double *grad_out, double *probe_ou
             std::vector<double> tmp(2 * n2);
             CK(cudaMemcpyAsync(tmp.data(), t.qacc.p, sizeof(double) * 2 * n2, cudaMemcpyDeviceToHost, s->st));
             CK(cudaStreamSynchronize(s->st));
-            const int n = s->n, r1 = s->plan.r1, r2 = n / r1;
+            const int n = s->n;
             double *o = probe_out + (size_t)j * 2 * n2;
             for (int ly = 0; ly < n; ++ly)
                 for (int lx = 0; lx < n; ++lx) {
-                    const int ky = ly / r1 + r2 * (ly % r1), kx = lx / r1 + r2 * (lx % r1);
+                    const int ky = scrambled_freq(ly, n, s->plan.ry1), kx = scrambled_freq(lx, n, s->plan.r1);
                     o[2 * ((size_t)ky * n + kx)] = tmp[2 * ((size_t)ly * n + lx)];
                     o[2 * ((size_t)ky * n + kx) + 1] = tmp[2 * ((size_t)ly * n + lx) + 1];
                 }

@@ -7,10 +7,13 @@
 namespace mset {
 
 // every compiled geometry; the first entry of a window size is its default,
-// the others are alternative thread shapes the autotuner may pick (at
-// n = 256 the default stages the adjoint's saved-wave rows by bulk copies:
-// 1.443 s against 1.474 s per pass of 3 large tilts on one B200)
-#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(64v2) X(96) X(96v2) X(128) X(128v2) X(128s) X(160) X(160v2) X(256s) X(256) X(256v2)
+// the others with the same scrambled layouts are alternative thread shapes
+// the autotuner may pick (at n = 256 the default stages the adjoint's
+// saved-wave rows by bulk copies: 1.443 s against 1.474 s per pass of 3 large
+// tilts on one B200).  At n = 128 the default is the three-phase shape; the
+// two-pass shape 128 after it has the layout of the sequential cluster
+// geometry 128c8 and serves the sequential entry points.
+#define MSET_GEOS(X) X(24) X(32) X(48) X(64) X(64v2) X(96) X(96v2) X(128t) X(128w) X(128) X(160) X(160v2) X(256s) X(256) X(256v2)
 #define X(N_) extern const GeoOps kGeo##N_;
 MSET_GEOS(X)
 #undef X
@@ -34,40 +37,10 @@ static const GeoOps *const kSeqGeos[] = {
 #undef X
 };
 
-bool plan_seq_for(int n, Plan *p) {
-    for (const GeoOps *g : kSeqGeos)
-        if (g->n == n) {
-            p->n = g->n;
-            p->r1 = g->r1;
-            p->nt = g->nt;
-            p->cl = g->cl;
-            p->staged = 0;
-            p->max_clusters = 0;
-            p->smem = g->smem;
-            p->ctas_per_sm = 0;
-            p->ops = g;
-            return true;
-        }
-    return false;
-}
-
-static const GeoOps *find_geo(int n, int variant) {
-    for (const GeoOps *g : kAllGeos)
-        if (g->n == n && variant-- == 0) return g;
-    return nullptr;
-}
-
-int plan_variants(int n) {
-    int c = 0;
-    for (const GeoOps *g : kAllGeos) c += g->n == n;
-    return c;
-}
-
-bool plan_for(int n, Plan *p, int variant) {
-    const GeoOps *g = find_geo(n, variant);
-    if (!g) return false;
+static void fill_plan(const GeoOps *g, Plan *p) {
     p->n = g->n;
     p->r1 = g->r1;
+    p->ry1 = g->ry1;
     p->nt = g->nt;
     p->cl = g->cl;
     p->staged = g->staged;
@@ -75,7 +48,56 @@ bool plan_for(int n, Plan *p, int variant) {
     p->smem = g->smem;
     p->ctas_per_sm = 0;
     p->ops = g;
+}
+
+bool plan_seq_for(int n, Plan *p) {
+    for (const GeoOps *g : kSeqGeos)
+        if (g->n == n) {
+            fill_plan(g, p);
+            p->staged = 0;
+            return true;
+        }
+    return false;
+}
+
+static bool same_layout(const GeoOps *a, const GeoOps *b) { return a->r1 == b->r1 && a->ry1 == b->ry1; }
+
+static const GeoOps *default_geo(int n) {
+    for (const GeoOps *g : kAllGeos)
+        if (g->n == n) return g;
+    return nullptr;
+}
+
+// the shapes of window n with the default's scrambled layouts, default first
+static const GeoOps *find_geo(int n, int variant) {
+    const GeoOps *d = default_geo(n);
+    if (!d) return nullptr;
+    for (const GeoOps *g : kAllGeos)
+        if (g->n == n && same_layout(g, d) && variant-- == 0) return g;
+    return nullptr;
+}
+
+int plan_variants(int n) {
+    const GeoOps *d = default_geo(n);
+    int c = 0;
+    for (const GeoOps *g : kAllGeos) c += d && g->n == n && same_layout(g, d);
+    return c;
+}
+
+bool plan_for(int n, Plan *p, int variant) {
+    const GeoOps *g = find_geo(n, variant);
+    if (!g) return false;
+    fill_plan(g, p);
     return true;
+}
+
+bool plan_for_layout(int n, int r1, int ry1, Plan *p) {
+    for (const GeoOps *g : kAllGeos)
+        if (g->n == n && g->r1 == r1 && g->ry1 == ry1) {
+            fill_plan(g, p);
+            return true;
+        }
+    return false;
 }
 
 int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,

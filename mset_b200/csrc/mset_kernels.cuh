@@ -76,7 +76,7 @@ __host__ __device__ inline int save_slots(int ns, int k) {
 
 // per-window-size kernel table (one translation unit per size, geo_<N>.cu)
 struct GeoOps {
-    int n, r1, nt;
+    int n, r1, ry1, nt;  // window, x residues, y residues of the scrambled layout, threads
     int cl;  // CTAs per field (thread-block cluster size; 1: one CTA per position)
     size_t smem;
     int staged;  // the adjoint's saved-wave rows are staged in shared memory by bulk copies
@@ -90,7 +90,7 @@ struct GeoOps {
 
 // host-side launchers (return cudaError_t as int)
 struct Plan {
-    int n, r1, nt;
+    int n, r1, ry1, nt;
     int cl;
     int staged;        // GeoOps::staged
     int max_clusters;  // cl > 1: clusters resident at once (0: unknown)
@@ -98,10 +98,15 @@ struct Plan {
     int ctas_per_sm;
     const GeoOps *ops;
 };
-// geometry `variant` (0: default) of window size n; plan_variants(n) of them exist
+// geometry `variant` (0: default) of window size n; plan_variants(n) of them
+// exist, all with the default's scrambled layouts
 bool plan_for(int n, Plan *p, int variant = 0);
+// the first geometry of window n whose scrambled layouts have r1 x residues
+// and ry1 y residues
+bool plan_for_layout(int n, int r1, int ry1, Plan *p);
 // the cluster geometry of window n for the sequential modes (kSeq, kStep),
-// when one is compiled; its scrambled layouts are plan_for(n)'s
+// when one is compiled (the sessions of those modes use the one-CTA shape with
+// its scrambled layouts, plan_for_layout)
 bool plan_seq_for(int n, Plan *p);
 int plan_variants(int n);
 int launch_positions(const Plan &pl, int method, int adjoint, int mode, const LaunchArgs &a, int grid,

@@ -146,14 +146,13 @@ struct L1FirstT {
 // kRows rows.  The first two iterations' rows are requested at the top of the
 // slab, two passes before they are read; iteration it + 2's rows as soon as
 // iteration it has read its stage.  The rows then cost a shared-memory load
-// instead of a global load held in registers across the task (16 registers
-// fewer at n = 128, and no spills).  Single-CTA fields only (a bulk copy of
-// whole contiguous rows), in the geometries compiled with STAGE (n = 128:
-// 2 stages x 2 rows x 1 KB x 16 warps = 64 KB beside the 139 KB field).
-// Measured on the mid workload it trades the global-load waits for
-// shared-memory queueing (long-scoreboard stalls per issue 1.49 -> 0.72,
-// MIO-throttle 0.74 -> 1.19) and is not faster than the register path, so it
-// is a variant the autotuner times, not the default.
+// instead of a global load held in registers across the task.  In the
+// geometries compiled with STAGE: the 256 x 256 cluster default (one bulk
+// copy per row, a CTA's consecutive local rows being 16 field rows apart),
+// where it removes most register spills (1.443 s against 1.474 s per pass of
+// 3 large tilts).  On the 128 x 128 two-pass shape it traded the global-load
+// waits for shared-memory queueing and was not faster (228.2 ms against
+// 225.6 ms per mid pass), so that window has no staged shape.
 template <class G>
 struct StageCfg {
     static constexpr int kRows = 32 % G::R1 == 0 ? 32 / G::R1 : 1;  // rows of one warp iteration
@@ -270,6 +269,7 @@ constexpr bool kColTw = G::R2 % 2 == 0;
 template <class G, int METHOD, int ADJ, int MODE>
 struct PositionKernel {
     static constexpr int N = G::N, NN = G::N * G::N, R1 = G::R1, R2 = G::R2;
+    static constexpr int CB = G::CB;  // points of a column-pass-B task
 
     // transmission of slab s at (y, x): exp(i sdz sum_{z in slab} V)
     // (mset.cu:134-153 / STEP02_FORWARD_4D.m:12-20; SSET: all z, mset.cu:391-404),
@@ -305,7 +305,7 @@ struct PositionKernel {
         }
         if constexpr (MODE == kBatchCentred) {
             const int h = (N + 1) / 2;
-            int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+            int r = G::scry(Ly) - h, c = G::scrx(Lx) - h;
             if (r < 0) r += N;
             if (c < 0) c += N;
             return sqrtf(__ldg(amp + (size_t)r * N + c));
@@ -322,19 +322,19 @@ struct PositionKernel {
         return __ldg(a.pscr + (size_t)Ly * N + Lx);
     }
 
-    // v[j] *= P(y0 + j, x) (CONJ: conj(P)) for the R1 rows of a column-pass-B
+    // v[j] *= P(y0 + j, x) (CONJ: conj(P)) for the CB rows of a column-pass-B
     // task.  Separable P: Px(x) is read once and Py two rows at a time
-    // (16-byte loads; y0 is a multiple of R1, the table 16-byte aligned),
+    // (16-byte loads; y0 is a multiple of CB, the table 16-byte aligned),
     // 9 shared-memory loads per task instead of 32 (-6% per mid pass)
     template <bool CONJ>
     static __device__ __forceinline__ void apply_prop(const LaunchArgs &a, const float2 *py, const float2 *px,
                                                       int y0, int x, float2 *v) {
-        static_assert(R1 % 2 == 0, "Py is read in pairs");
+        static_assert(CB % 2 == 0, "Py is read in pairs");
         if (a.psep) {
             const float2 pxv = px[x];
             const float4 *q4 = reinterpret_cast<const float4 *>(py + y0);
 #pragma unroll
-            for (int m = 0; m < R1 / 2; ++m) {
+            for (int m = 0; m < CB / 2; ++m) {
                 const float4 q = q4[m];
                 const float2 p0 = cmul(make_float2(q.x, q.y), pxv), p1 = cmul(make_float2(q.z, q.w), pxv);
                 v[2 * m] = CONJ ? cmulc(v[2 * m], p0) : cmul(v[2 * m], p0);
@@ -342,7 +342,7 @@ struct PositionKernel {
             }
         } else {
 #pragma unroll
-            for (int j = 0; j < R1; ++j) {
+            for (int j = 0; j < CB; ++j) {
                 const float2 p = prop(a, py, px, y0 + j, x);
                 v[j] = CONJ ? cmulc(v[j], p) : cmul(v[j], p);
             }
@@ -367,17 +367,13 @@ struct PositionKernel {
             });
         sync_rows();
         for (int s = s0; s < s1; ++s) {
-            row_passB<G, -1>(buf);
-            sync_rowcol();
-            col_passA<G, -1, true, kColTw<G>>(buf, tw);
+            mid_fwd<G, -1, kColTw<G>>(buf, tw);
             sync_cols<G>();
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
                 apply_prop<false>(a, py, px, y0, x, v);
             });
             sync_cols<G>();
-            col_passA<G, +1, false, kColTw<G>>(buf, tw);
-            sync_rowcol();
-            row_passB<G, +1>(buf);
+            mid_inv<G, +1, kColTw<G>>(buf, tw);
             sync_rows();
             float2 *o = out + (size_t)(s - s0) * NN;
             auto store = [&](int y, int n1, float2 *v) {
@@ -435,11 +431,10 @@ struct PositionKernel {
         const float s1 = syp - a.center, s2 = sxp - a.center;  // mset.cu:121
         // separable Fourier shift factor, indexed by scrambled location
         for (int L = threadIdx.x; L < N; L += G::NT) {
-            const float nf = shift_grid(G::scr(L), N);
             float sn, cs;
-            sincosf(2.0f * MSET_REF_PI * (s1 * nf / (float)N), &sn, &cs);
+            sincosf(2.0f * MSET_REF_PI * (s1 * shift_grid(G::scry(L), N) / (float)N), &sn, &cs);
             e1[L] = make_float2(cs, sn);
-            sincosf(2.0f * MSET_REF_PI * (s2 * nf / (float)N), &sn, &cs);
+            sincosf(2.0f * MSET_REF_PI * (s2 * shift_grid(G::scrx(L), N) / (float)N), &sn, &cs);
             e2[L] = make_float2(cs, sn);
         }
         sync_all<G>();
@@ -467,12 +462,10 @@ struct PositionKernel {
             const float2 *q = t.Q + (size_t)y0 * N + x;
             const float2 ex = e2[x];
 #pragma unroll
-            for (int j = 0; j < R1; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
+            for (int j = 0; j < CB; ++j) v[j] = cmul(cmul(q[(size_t)j * N], e1[y0 + j]), ex);
         });
         sync_cols<G>();
-        col_passA<G, -1, false, kColTw<G>>(buf, tw);
-        sync_rowcol();
-        row_passB<G, -1>(buf);
+        mid_inv<G, -1, kColTw<G>>(buf, tw);
         sync_rows();
         row_passA_pf<G, -1, -1, TPre<G>>(buf, tw, pf_t(0), [&](int y, int n1, float2 *v, const TPre<G> &pre) {
             if constexpr (MODE != kSim && MODE != kErr) {
@@ -490,17 +483,13 @@ struct PositionKernel {
             for (int s = 0; s < ns; ++s) {
                 if (Tslab && s + 1 < ns)
                     l1_first<G>(L1FirstT<G>{reinterpret_cast<const char *>(Tslab + (size_t)(s + 1) * NN)});
-                row_passB<G, -1>(buf);
-                sync_rowcol();
-                col_passA<G, -1, true, kColTw<G>>(buf, tw);
+                mid_fwd<G, -1, kColTw<G>>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
                     apply_prop<false>(a, py, px, y0, x, v);
                 });
                 sync_cols<G>();
-                col_passA<G, +1, false, kColTw<G>>(buf, tw);
-                sync_rowcol();
-                row_passB<G, +1>(buf);
+                mid_inv<G, +1, kColTw<G>>(buf, tw);
                 sync_rows();
                 const bool last = s + 1 == ns;
                 const int sn = last ? s : s + 1;
@@ -546,21 +535,19 @@ struct PositionKernel {
             // adjoint's bulk copies read them through the async proxy
             asm volatile("fence.proxy.async.global;" ::: "memory");
         }
-        row_passB<G, -1>(buf);
-        sync_rowcol();
-        col_passA<G, -1, true, kColTw<G>>(buf, tw);
+        mid_fwd<G, -1, kColTw<G>>(buf, tw);
         sync_cols<G>();
         const float *amp = t.amp ? t.amp + (size_t)p * NN : nullptr;
         const unsigned short *ampb = t.ampb ? t.ampb + (size_t)p * NN : nullptr;
         if constexpr (MODE == kSim || MODE == kErr) {
             col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-                for (int j = 0; j < R1; ++j) {
+                for (int j = 0; j < CB; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     if constexpr (MODE == kSim) {
                         // centred (MATLAB) layout: row r with (r + ceil(N/2)) mod N = ky
                         const int h = (N + 1) / 2;
-                        int r = G::scr(y0 + j) - h, c = G::scr(x) - h;
+                        int r = G::scry(y0 + j) - h, c = G::scrx(x) - h;
                         if (r < 0) r += N;
                         if (c < 0) c += N;
                         t.inten[(size_t)p * NN + (size_t)r * N + c] = a2;
@@ -584,7 +571,7 @@ struct PositionKernel {
             // |Psi|^2 (centred) out, error sum; the waves stay in the slots
             col_passB<G, -1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-                for (int j = 0; j < R1; ++j) {
+                for (int j = 0; j < CB; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     const float A = sqrtf(a2 + 1e-30f);
                     const float M = meas_amp(amp, ampb, y0 + j, x);
@@ -592,7 +579,7 @@ struct PositionKernel {
                     err += (double)(d * d);
                     a.step_resi[(size_t)(y0 + j) * N + x] = cscale(v[j], 1.0f - M / A);
                     const int h = (N + 1) / 2;
-                    int r = G::scr(y0 + j) - h, c = G::scr(x) - h;
+                    int r = G::scry(y0 + j) - h, c = G::scrx(x) - h;
                     if (r < 0) r += N;
                     if (c < 0) c += N;
                     a.step_calc[(size_t)r * N + c] = a2;
@@ -606,7 +593,7 @@ struct PositionKernel {
         } else {
             col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-                for (int j = 0; j < R1; ++j) {
+                for (int j = 0; j < CB; ++j) {
                     const float a2 = v[j].x * v[j].x + v[j].y * v[j].y;
                     const float A = sqrtf(a2 + 1e-30f);
                     const float M = meas_amp(amp, ampb, y0 + j, x);
@@ -628,7 +615,7 @@ struct PositionKernel {
             // (SSET: r / N^2), inverse column transform started
             col_passB<G, 0, +1>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-                for (int j = 0; j < R1; ++j) {
+                for (int j = 0; j < CB; ++j) {
                     const float2 r = a.step_resi[(size_t)(y0 + j) * N + x];
                     if constexpr (METHOD == kMSET) v[j] = cmulc(r, prop(a, py, px, y0 + j, x));
                     else v[j] = cscale(r, 1.0f / (float)NN);
@@ -677,9 +664,7 @@ struct PositionKernel {
                                   wave, Own<G>::warp() * Own<G>::RPW, G::ybase(), stage_phase, a.fault};
                 stg.start();
             }
-            col_passA<G, +1, false, kColTw<G>>(buf, tw);
-            sync_rowcol();
-            row_passB<G, +1>(buf);
+            mid_inv<G, +1, kColTw<G>>(buf, tw);
             sync_rows();
             // the operands are loaded before the task's shared-memory reads:
             // loading them inside the op instead (fewer live registers at
@@ -772,9 +757,7 @@ struct PositionKernel {
             if (s > 0) {
                 run_rowA(std::integral_constant<int, -1>{});
                 sync_rows();
-                row_passB<G, -1>(buf);
-                sync_rowcol();
-                col_passA<G, -1, true, kColTw<G>>(buf, tw);
+                mid_fwd<G, -1, kColTw<G>>(buf, tw);
                 sync_cols<G>();
                 col_passB<G, -1, +1>(buf, [&](int y0, int x, float2 *v) {
                     apply_prop<true>(a, py, px, y0, x, v);
@@ -815,9 +798,7 @@ struct PositionKernel {
         //      F^{-1}(probe) domain (mset.cu:288-312) ----
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         sync_rows();
-        row_passB<G, +1>(buf);
-        sync_rowcol();
-        col_passA<G, +1, true, kColTw<G>>(buf, tw);
+        mid_fwd<G, +1, kColTw<G>>(buf, tw);
         sync_cols<G>();
         const float inv = 1.0f / (float)NN;
         // descriptor fields in registers: the atomics below go through generic
@@ -826,16 +807,16 @@ struct PositionKernel {
         double *const qacc = t.qacc;
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
             const float2 ex = e2[x];
-            const float kx = 2.0f * MSET_REF_PI * shift_grid(G::scr(x), N) / (float)N;
+            const float kx = 2.0f * MSET_REF_PI * shift_grid(G::scrx(x), N) / (float)N;
 #pragma unroll
-            for (int j = 0; j < R1; ++j) {
+            for (int j = 0; j < CB; ++j) {
                 const size_t li = (size_t)(y0 + j) * N + x;
                 const float2 fs = cmul(e1[y0 + j], ex);
                 const float2 d = cscale(cmulc(v[j], fs), inv);
                 if constexpr (ADJ == kEXACT) {
                     // spectral derivative of psi0 w.r.t. the scan coordinates
                     const float2 qf = cmul(Qd[li], fs);
-                    const float ky = 2.0f * MSET_REF_PI * shift_grid(G::scr(y0 + j), N) / (float)N;
+                    const float ky = 2.0f * MSET_REF_PI * shift_grid(G::scry(y0 + j), N) / (float)N;
                     // X = Q fs (i kappa); -Re(conj(X) Y)
                     const float2 Xx = make_float2(-qf.y * kx, qf.x * kx);
                     const float2 Xy = make_float2(-qf.y * ky, qf.x * ky);
@@ -897,8 +878,14 @@ __device__ __forceinline__ void load_tables(float2 *buf, const LaunchArgs &a) {
     float2 *px = buf + Smem<G>::PX;
     float2 *twt = buf + Smem<G>::TWT;
     for (int i = threadIdx.x; i < G::N; i += G::NT) {
-        tw[i] = a.twn[i];
-        twt[(i % G::R1) * G::R2 + i / G::R1] = a.twn[i];  // [k2][n1] -> [n1][k2]
+        if constexpr (G::THREE) {
+            // the x table [a][k1] and the y table [k1'][b] of phase 2
+            tw[i] = a.twn[i];
+            twt[i] = a.twn[G::N + i];
+        } else {
+            tw[i] = a.twn[i];
+            twt[(i % G::R1) * G::R2 + i / G::R1] = a.twn[i];  // [k2][n1] -> [n1][k2]
+        }
         if (a.psep) {
             py[i] = a.psep[i];
             px[i] = a.psep[G::N + i];
@@ -981,7 +968,7 @@ __global__ void k_prep_amp(const float *meas, float *amp, long npos) {
         const long p = i / ((long)G::N * G::N);
         const int l = (int)(i % ((long)G::N * G::N));
         const int Ly = l / G::N, Lx = l % G::N;
-        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        int r = G::scry(Ly) - h, c = G::scrx(Lx) - h;
         if (r < 0) r += G::N;
         if (c < 0) c += G::N;
         amp[i] = sqrtf(meas[p * G::N * G::N + (long)r * G::N + c]);
@@ -997,7 +984,7 @@ __global__ void k_prep_amp_bf16(const float *meas, unsigned short *ib, long npos
         const long p = i / ((long)G::N * G::N);
         const int l = (int)(i % ((long)G::N * G::N));
         const int Ly = l / G::N, Lx = l % G::N;
-        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        int r = G::scry(Ly) - h, c = G::scrx(Lx) - h;
         if (r < 0) r += G::N;
         if (c < 0) c += G::N;
         const __nv_bfloat16 v = __float2bfloat16_rn(meas[p * G::N * G::N + (long)r * G::N + c]);
@@ -1012,7 +999,7 @@ __global__ void k_prep_prop(const float2 *prop, float2 *pscr) {
     const float inv = 1.0f / (float)(G::N * G::N);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G::N * G::N; i += gridDim.x * blockDim.x) {
         const int Ly = i / G::N, Lx = i % G::N;
-        int r = G::scr(Ly) - h, c = G::scr(Lx) - h;
+        int r = G::scry(Ly) - h, c = G::scrx(Lx) - h;
         if (r < 0) r += G::N;
         if (c < 0) c += G::N;
         pscr[i] = cscale(prop[r * G::N + c], inv);
@@ -1026,7 +1013,7 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
     extern __shared__ __align__(16) float2 smem[];
     float2 *buf = smem;
     float2 *tw = buf + G::FIELD;
-    for (int i = threadIdx.x; i < G::N; i += G::NT) tw[i] = twn[i];
+    for (int i = threadIdx.x; i < (G::THREE ? 2 : 1) * G::N; i += G::NT) tw[i] = twn[i];
     sync_all<G>();  // (cluster) every CTA has started before any remote access
     constexpr int N = G::N;
     const int yb = G::ybase();
@@ -1036,24 +1023,20 @@ __global__ void __launch_bounds__(G::NT) k_probe_q(const float2 *in, float2 *out
         __syncthreads();
         row_passA<G, 0, +1>(buf, tw, NoOp{});
         __syncthreads();
-        row_passB<G, +1>(buf);
-        sync_rowcol();
-        col_passA<G, +1, true>(buf, tw);
+        mid_fwd<G, +1, false>(buf, tw);
         sync_all<G>();
         const float inv = 1.0f / (float)(N * N);
         col_passB<G, +1, 0>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-            for (int j = 0; j < G::R1; ++j) out[(size_t)(y0 + j) * N + x] = cscale(v[j], inv);
+            for (int j = 0; j < G::CB; ++j) out[(size_t)(y0 + j) * N + x] = cscale(v[j], inv);
         });
     } else {
         col_passB<G, 0, -1>(buf, [&](int y0, int x, float2 *v) {
 #pragma unroll
-            for (int j = 0; j < G::R1; ++j) v[j] = in[(size_t)(y0 + j) * N + x];
+            for (int j = 0; j < G::CB; ++j) v[j] = in[(size_t)(y0 + j) * N + x];
         });
         sync_all<G>();
-        col_passA<G, -1, false>(buf, tw);
-        sync_rowcol();
-        row_passB<G, -1>(buf);
+        mid_inv<G, -1, false>(buf, tw);
         __syncthreads();
         row_passA<G, -1, 0>(buf, tw, [&](int y, int n1, float2 *v) {
 #pragma unroll
@@ -1201,6 +1184,7 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
     using SeqGeo##NAME_ = GeoCl<N_, R1_, NT_, CL_>;                                    \
     extern const GeoOps kSeqGeo##NAME_ = {N_,                                          \
                                           R1_,                                         \
+                                          SeqGeo##NAME_::RY1,                          \
                                           SeqGeo##NAME_::NT,                           \
                                           SeqGeo##NAME_::CL,                           \
                                           smem_bytes<SeqGeo##NAME_>(),                 \
@@ -1219,12 +1203,15 @@ int geo_probe_q(bool to_q, const float2 *in, float2 *out, const float2 *twn, cud
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_, 1, true>))
 #define MSET_DEFINE_GEO_CL_VARIANT(NAME_, N_, R1_, NT_, CL_, MINB_) \
     MSET_DEFINE_GEO_T(NAME_, N_, R1_, (GeoCl<N_, R1_, NT_, CL_, MINB_>))
+// the three-phase shape of the 128 x 128 window (Geo3; WIDE_: 16-byte phase-2 accesses)
+#define MSET_DEFINE_GEO3(NAME_, WIDE_) MSET_DEFINE_GEO_T(NAME_, 128, 8, (Geo3<1, WIDE_>))
 #define MSET_UNPAREN(...) __VA_ARGS__
 #define MSET_DEFINE_GEO_T(NAME_, N_, R1_, GT_)                                         \
     namespace mset {                                                                   \
     using Geo##NAME_ = MSET_UNPAREN GT_;                                               \
     extern const GeoOps kGeo##NAME_ = {N_,                                             \
                                        R1_,                                            \
+                                       Geo##NAME_::RY1,                                \
                                        Geo##NAME_::NT,                                 \
                                        Geo##NAME_::CL,                                 \
                                        smem_bytes<Geo##NAME_>(),                       \

@@ -109,7 +109,7 @@ def test_batched_gradient_matches_oracle(gpu_available, admode, method, n):
                                       sigma=c0["sigma"], dz=c0["dz"], binning=2, method=method, adjoint=admode)
         assert rel_l2(out["grad"][j], g) < TOL
         assert rel_l2(np.fft.fft2(out["probe"][j]), pa) < TOL
-        assert rel_l2(out["posdir"][5 * j:5 * j + 5], pd) < (TOL if n <= 96 else 3e-4 if n <= 160 else pos_tol(n))
+        assert rel_l2(out["posdir"][5 * j:5 * j + 5], pd) < pos_tol(n)
         assert abs(out["err"][j] - e) <= TOL * e
 
 
