@@ -605,11 +605,23 @@ def cpu_baseline(args, cfg, spec) -> dict:
         host_pass(smp, cores)
         reps += 1
     dt = time.perf_counter() - t0
+    # the reference-semantics pass on one thread (positions in order, each
+    # updating the volume, probe and its coordinates before the next)
+    ks = min(16, k)
+    t1 = time.perf_counter()
+    O.sequential_tilt_fp32(smp["V"], smp["spec"].probe, smp["spec"].prop, smp["sx"][:ks], smp["sy"][:ks],
+                           smp["meas"][:ks], sigma=smp["spec"].sigma, dz=smp["cfg"].dx, step=(1e-3, 1e-6, 1e-3),
+                           binning=smp["cfg"].slice_binning)
+    dts = time.perf_counter() - t1
     return {"value": reps * k * ns / dt, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
             "dtype": "fp32",
             "sample": f"{reps} pass(es) over {k} positions of the 0-degree tilt of the same geometry ({ns} slabs "
                       f"each), single-precision C port of the reference's CPU path (its MATLAB STEP02/STEP03 run "
-                      f"in single), {dt:.1f} s"}
+                      f"in single), {dt:.1f} s",
+            "sequential": {"value": ks * ns / dts, "unit": "slice-propagations/s", "cores": 1,
+                           "sample": f"{ks} positions of the same sample in order with per-position updates "
+                                     f"(run_main_mset semantics), single-precision C port on one thread, "
+                                     f"{dts:.1f} s"}}
 
 
 def run_reference(args):

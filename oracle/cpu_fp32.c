@@ -21,6 +21,12 @@
  * per call (the batched method's order); positions run in parallel over
  * OpenMP threads, each with its own float gradient buffer.
  *
+ * cpu32_sequential_tilt is the same position in the reference's own order
+ * (run_main_mset, mset.cu:80-334; Run_MSET_recon.m:136-157 on the CPU path):
+ * one position after the other on one thread, each starting from the volume,
+ * probe and coordinates the previous ones updated, with the transmission
+ * rebuilt from the current volume per position (mset.cu:134-153).
+ *
  * FFT: iterative radix-2 (window edge a power of two), twiddles computed in
  * double and stored as float.
  */
@@ -352,6 +358,132 @@ int cpu32_simulate(int n, int nz, int binning, double sigma, double dz, int npos
     free(P);
     free(Q);
     free(T);
+    plan32_free(&pl);
+    return 0;
+}
+
+/* Sequential tilt pass with reference semantics (MSET, reference adjoint
+ * formula), single precision on one thread: for each position in order the
+ * forward and adjoint of cpu32_batched_tilt, then RVol += step0 Re(g)
+ * replicated over each slab's voxels (mset.cu:265-284), probe -= step1
+ * F(F^{-1}(chi0) fs(-s)) (mset.cu:288-312), scan coordinates += step2 times
+ * the finite-difference position direction (mset.cu:316-327).  rvol, probe,
+ * scan_x, scan_y are updated in place; err_sum receives sum_p sum_px
+ * (A - M)^2.  Sums over pixels (error, position direction) in double. */
+int cpu32_sequential_tilt(int n, int nz, int binning, double sigma, double dz, const double *step, int npos,
+                          float *rvol, float *probe, const float *prop_centred, float *scan_x, float *scan_y,
+                          const float *measured, double *err_sum) {
+    if (n < 2 || nz <= 0 || binning <= 0 || npos < 0) return -1;
+    plan32 pl;
+    if (plan32_init(&pl, n)) return -1;
+    const size_t n2 = (size_t)n * n;
+    const int ns = (nz + binning - 1) / binning;
+    cf *P = malloc(sizeof(cf) * n2), *T = malloc(sizeof(cf) * n2 * ns), *Q = malloc(sizeof(cf) * n2);
+    cf *w = malloc(sizeof(cf) * n2), *fs = malloc(sizeof(cf) * n2), *psi0 = malloc(sizeof(cf) * n2);
+    cf *waves = malloc(sizeof(cf) * n2 * (ns + 1)), *line = malloc(sizeof(cf) * n), *d = malloc(sizeof(cf) * n2);
+    float *g = malloc(sizeof(float) * n2 * ns);
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) {
+            const size_t i = (size_t)r * n + c;
+            P[ishift(r, c, n)] = prop_centred[2 * i] + I * prop_centred[2 * i + 1];
+        }
+    const float sdz = (float)(sigma * dz);
+    const float center = roundf((n + 1.0f) / 2.0f);
+    const float st0 = (float)step[0], st1 = (float)step[1], st2 = (float)step[2];
+    double err_total = 0.0;
+    for (int p = 0; p < npos; ++p) {
+        for (int s = 0; s < ns; ++s) { /* transmission from the current volume (mset.cu:134-153) */
+            const int z0 = s * binning, z1 = z0 + binning < nz ? z0 + binning : nz;
+            for (size_t i = 0; i < n2; ++i) {
+                float acc = 0.f;
+                for (int z = z0; z < z1; ++z) acc += rvol[(size_t)z * n2 + i];
+                T[(size_t)s * n2 + i] = cosf(sdz * acc) + I * sinf(sdz * acc);
+            }
+        }
+        /* psi0 = F(F^{-1}(probe) fs) with the current probe (mset.cu:110-131) */
+        for (size_t i = 0; i < n2; ++i) Q[i] = probe[2 * i] + I * probe[2 * i + 1];
+        ifft2n(&pl, Q, line);
+        const float s1 = scan_y[p] - center, s2 = scan_x[p] - center;
+        shift_factor(n, s1, s2, fs);
+        for (size_t i = 0; i < n2; ++i) psi0[i] = Q[i] * fs[i];
+        fft2(&pl, psi0, -1, line);
+        memcpy(w, psi0, sizeof(cf) * n2);
+        for (int s = 0; s < ns; ++s) { /* mset.cu:157-183 */
+            const cf *Ts = T + (size_t)s * n2;
+            for (size_t i = 0; i < n2; ++i) w[i] *= Ts[i];
+            fft2(&pl, w, -1, line);
+            for (size_t i = 0; i < n2; ++i) w[i] *= P[i];
+            ifft2n(&pl, w, line);
+            memcpy(waves + (size_t)(s + 1) * n2, w, sizeof(cf) * n2);
+        }
+        fft2(&pl, w, -1, line); /* far field, residual (mset.cu:186-227) */
+        const float *meas = measured + (size_t)p * n2;
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) {
+                const size_t k = ishift(r, c, n);
+                const float a2 = crealf(w[k]) * crealf(w[k]) + cimagf(w[k]) * cimagf(w[k]);
+                const float A = sqrtf(a2 + 1e-30f), M = sqrtf(meas[(size_t)r * n + c]);
+                err_total += (double)((A - M) * (A - M));
+                w[k] *= 1.0f - M / A;
+            }
+        for (int s = ns - 1; s >= 0; --s) { /* mset.cu:232-271 */
+            const cf *Ts = T + (size_t)s * n2;
+            const cf *psi = waves + (size_t)(s + 1) * n2; /* mset.cu:248-251 */
+            for (size_t i = 0; i < n2; ++i) w[i] *= conjf(P[i]);
+            ifft2n(&pl, w, line);
+            float *gs = g + (size_t)s * n2;
+            for (size_t i = 0; i < n2; ++i) {
+                gs[i] = crealf(I * conjf(Ts[i]) * conjf(psi[i]) * w[i]);
+                w[i] *= conjf(Ts[i]);
+            }
+            if (s > 0) fft2(&pl, w, -1, line);
+        }
+        /* position direction from conj(psi0) and chi0 (utility.cu:829-876) */
+        double px = 0.0, py = 0.0;
+        for (int i1 = 0; i1 < n; ++i1)
+            for (int i2 = 0; i2 < n; ++i2) {
+                const size_t i = (size_t)i1 * n + i2;
+                const cf *f = psi0;
+                cf dx, dy;
+                if (i2 == 0) dx = conjf(f[i + 1]) - conjf(f[i]);
+                else if (i2 == n - 1) dx = conjf(f[i]) - conjf(f[i - 1]);
+                else dx = (conjf(f[i + 1]) - conjf(f[i - 1])) * 0.5f;
+                if (i1 == 0) dy = conjf(f[i + n]) - conjf(f[i]);
+                else if (i1 == n - 1) dy = conjf(f[i]) - conjf(f[i - n]);
+                else dy = (conjf(f[i + n]) - conjf(f[i - n])) * 0.5f;
+                px += (double)crealf(dx * w[i]);
+                py += (double)crealf(dy * w[i]);
+            }
+        /* probe direction F(F^{-1}(chi0) fs(-s)) and the probe update (mset.cu:288-312) */
+        memcpy(d, w, sizeof(cf) * n2);
+        ifft2n(&pl, d, line);
+        for (size_t i = 0; i < n2; ++i) d[i] *= conjf(fs[i]);
+        fft2(&pl, d, -1, line);
+        for (size_t i = 0; i < n2; ++i) {
+            probe[2 * i] -= st1 * crealf(d[i]);
+            probe[2 * i + 1] -= st1 * cimagf(d[i]);
+        }
+        /* object update, slab-replicated (mset.cu:265-284) */
+        for (int s = 0; s < ns; ++s) {
+            const int z0 = s * binning, z1 = z0 + binning < nz ? z0 + binning : nz;
+            const float *gs = g + (size_t)s * n2;
+            for (int z = z0; z < z1; ++z)
+                for (size_t i = 0; i < n2; ++i) rvol[(size_t)z * n2 + i] += st0 * gs[i];
+        }
+        scan_x[p] += st2 * (float)px; /* mset.cu:322 */
+        scan_y[p] += st2 * (float)py; /* mset.cu:327 */
+    }
+    *err_sum = err_total;
+    free(P);
+    free(T);
+    free(Q);
+    free(w);
+    free(fs);
+    free(psi0);
+    free(waves);
+    free(line);
+    free(d);
+    free(g);
     plan32_free(&pl);
     return 0;
 }

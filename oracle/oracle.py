@@ -161,6 +161,8 @@ def lib32() -> C.CDLL:
                                          _F, _F, _F, _D, _D, _D, _D, C.c_int]
         L.cpu32_simulate.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _F, _F, _F, _F,
                                      _F, _F, C.c_int]
+        L.cpu32_sequential_tilt.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _D, C.c_int, _F,
+                                            _F, _F, _F, _F, _F, _D]
         _lib32 = L
     return _lib32
 
@@ -187,6 +189,27 @@ def batched_tilt_fp32(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz,
     if rc != 0:
         raise ValueError("cpu_fp32: the window must be a power of two")
     return g, pa[..., 0] + 1j * pa[..., 1], pd, float(err[0])
+
+
+def sequential_tilt_fp32(rvol, probe, prop, scan_x, scan_y, measured, *, sigma, dz, step, binning=1):
+    """The reference-semantics tilt pass (run_main_mset) in single precision on
+    one thread (cpu_fp32.c): returns the updated (rvol, probe, scan_x,
+    scan_y) and the error sum, as run_tilt does in FP64."""
+    rv = np.array(rvol, dtype=np.float32, order="C")
+    nz, n, _ = rv.shape
+    pr = np.array(probe, dtype=np.complex64, order="C")
+    pp = np.ascontiguousarray(prop, dtype=np.complex64)
+    sx = np.array(scan_x, dtype=np.float32)
+    sy = np.array(scan_y, dtype=np.float32)
+    me = np.ascontiguousarray(measured, dtype=np.float32)
+    st = np.asarray(step, dtype=np.float64)
+    err = np.zeros(1)
+    rc = lib32().cpu32_sequential_tilt(n, nz, binning, sigma, dz, _d(st), sx.size, _f(rv),
+                                       pr.view(np.float32).ctypes.data_as(_F), pp.view(np.float32).ctypes.data_as(_F),
+                                       _f(sx), _f(sy), _f(me), _d(err))
+    if rc != 0:
+        raise ValueError("cpu_fp32: the window must be a power of two")
+    return rv, pr, sx, sy, float(err[0])
 
 
 def _rot_setup():
