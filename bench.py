@@ -643,7 +643,6 @@ def run_reference(args):
         host_pass(smp, cores)
     dt = (time.perf_counter() - t0) / args.steps
     value = k * ns / dt
-    nz, ny, nx = cfg.vol
     line = {
         "impl": "reference",
         "metric": "slice-propagations/s (fwd+adjoint)",
@@ -658,9 +657,10 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic",
-        "config": {"workload": f"{cfg.name}: {nx}x{ny}x{nz} volume, {cfg.window}^2 window, "
-                               f"{cfg.scan[0]}x{cfg.scan[1]} scan, {cfg.n_tilts} tilts, {ns} slabs x "
-                               f"{cfg.slice_binning} voxels (sampled: {k} positions of the 0-degree tilt per step)"},
+        "config": {"workload": workload_name(cfg, ns, smp["spec"].scan_x.size * cfg.n_tilts),
+                   "positions": smp["spec"].scan_x.size * cfg.n_tilts, "slabs": ns, "window": cfg.window,
+                   "units_per_step": smp["spec"].scan_x.size * cfg.n_tilts * ns,
+                   "sampled": f"{k} positions of the 0-degree tilt per step (units/s of the sample)"},
         "cpu_baseline": {"value": value, "unit": "slice-propagations/s", "cores": cores, "kind": "port",
                          "sample": f"{k} positions x {ns} slabs per step; the reference's CPU path is MATLAB "
                                    "code (STEP02/STEP03) in single precision, unavailable on this box, so its "
