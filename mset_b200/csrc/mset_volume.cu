@@ -6,7 +6,9 @@
 //
 // All stencils are periodic (MATLAB circshift).  Volumes are C order
 // [n3][n2][n1] = MATLAB (n1, n2, n3); MATLAB dim 1 is the fastest axis.
-// HBM/L2-bound elementwise work: grid-stride loops over 148 x 8 CTAs.
+// HBM/L2-bound elementwise work: grid-stride loops over 148 x 8 CTAs (the
+// TV stencils: over rows, one CTA per row).
+#include <algorithm>
 #include <cmath>
 
 #include "mset_volume.cuh"
@@ -23,69 +25,96 @@ inline int grid_for(long total) {
 
 __device__ __forceinline__ long wrap(long i, long n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// The TV stencils run one CTA per row (i2, i3) of the volume in a
+// grid-stride loop over rows, threads over i1: the periodic neighbours' rows
+// are found once per row (one 32-bit division) instead of three 64-bit
+// divisions per element, which made these kernels integer-bound.
+struct Rows {
+    int n1, n2, n3;
+    long V;
+    // first element of row (i2, i3); neighbour rows with periodic wrap
+    __device__ __forceinline__ long at(int i2, int i3) const { return ((long)i3 * n2 + i2) * n1; }
+};
+
 // D = TV_div(Y) - in / lambda   (the argument of TV_del in TV_method.m:21)
-__global__ void k_tv_d(const float *Y, const float *in, float *D, int n1, int n2, int n3, float inv_lam) {
-    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
-    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
-        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
-        const long m1 = r - i1 + wrap(i1 - 1, n1);
-        const long m2 = r + (wrap(i2 - 1, n2) - i2) * s2;
-        const long m3 = r + (wrap(i3 - 1, n3) - i3) * s3;
-        const float d = Y[r] + Y[V + r] + Y[2 * V + r] - Y[m1] - Y[V + m2] - Y[2 * V + m3];
-        D[r] = d - in[r] * inv_lam;
+__global__ void k_tv_d(const float *Y, const float *in, float *D, Rows g, float inv_lam) {
+    const long V = g.V;
+    for (int row = blockIdx.x; row < g.n2 * g.n3; row += gridDim.x) {
+        const int i2 = row % g.n2, i3 = row / g.n2;
+        const long b = g.at(i2, i3), b2 = g.at(i2 == 0 ? g.n2 - 1 : i2 - 1, i3),
+                   b3 = g.at(i2, i3 == 0 ? g.n3 - 1 : i3 - 1);
+        for (int i1 = threadIdx.x; i1 < g.n1; i1 += blockDim.x) {
+            const long r = b + i1;
+            const int i1m = i1 == 0 ? g.n1 - 1 : i1 - 1;
+            const float d = Y[r] + Y[V + r] + Y[2 * V + r] - Y[b + i1m] - Y[V + b2 + i1] - Y[2 * V + b3 + i1];
+            D[r] = d - in[r] * inv_lam;
+        }
     }
 }
 
 // P <- TV_project(src + tau TV_del(D)); FISTA: Y <- P + m (P - P_old) in FP64
-__global__ void k_tv_step(float *P, float *Y, const float *D, int n1, int n2, int n3, float tau, double m,
-                          int fista) {
-    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
-    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
-        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
-        const float d0 = D[r];
-        const float t1 = tau * (D[r - i1 + wrap(i1 + 1, n1)] - d0);
-        const float t2 = tau * (D[r + (wrap(i2 + 1, n2) - i2) * s2] - d0);
-        const float t3 = tau * (D[r + (wrap(i3 + 1, n3) - i3) * s3] - d0);
-        const float *src = fista ? Y : P;
-        const float q1 = src[r] + t1, q2 = src[V + r] + t2, q3 = src[2 * V + r] + t3;
-        const float nrm = sqrtf(fmaxf(1.0f, q1 * q1 + q2 * q2 + q3 * q3));
-        const float p1 = q1 / nrm, p2 = q2 / nrm, p3 = q3 / nrm;
-        if (fista) {
-            const double o1 = P[r], o2 = P[V + r], o3 = P[2 * V + r];
-            Y[r] = (float)(p1 + m * (p1 - o1));
-            Y[V + r] = (float)(p2 + m * (p2 - o2));
-            Y[2 * V + r] = (float)(p3 + m * (p3 - o3));
+__global__ void k_tv_step(float *P, float *Y, const float *D, Rows g, float tau, double m, int fista) {
+    const long V = g.V;
+    for (int row = blockIdx.x; row < g.n2 * g.n3; row += gridDim.x) {
+        const int i2 = row % g.n2, i3 = row / g.n2;
+        const long b = g.at(i2, i3), b2 = g.at(i2 == g.n2 - 1 ? 0 : i2 + 1, i3),
+                   b3 = g.at(i2, i3 == g.n3 - 1 ? 0 : i3 + 1);
+        for (int i1 = threadIdx.x; i1 < g.n1; i1 += blockDim.x) {
+            const long r = b + i1;
+            const int i1p = i1 == g.n1 - 1 ? 0 : i1 + 1;
+            const float d0 = D[r];
+            const float t1 = tau * (D[b + i1p] - d0);
+            const float t2 = tau * (D[b2 + i1] - d0);
+            const float t3 = tau * (D[b3 + i1] - d0);
+            const float *src = fista ? Y : P;
+            const float q1 = src[r] + t1, q2 = src[V + r] + t2, q3 = src[2 * V + r] + t3;
+            const float nrm = sqrtf(fmaxf(1.0f, q1 * q1 + q2 * q2 + q3 * q3));
+            const float p1 = q1 / nrm, p2 = q2 / nrm, p3 = q3 / nrm;
+            if (fista) {
+                const double o1 = P[r], o2 = P[V + r], o3 = P[2 * V + r];
+                Y[r] = (float)(p1 + m * (p1 - o1));
+                Y[V + r] = (float)(p2 + m * (p2 - o2));
+                Y[2 * V + r] = (float)(p3 + m * (p3 - o3));
+            }
+            P[r] = p1;
+            P[V + r] = p2;
+            P[2 * V + r] = p3;
         }
-        P[r] = p1;
-        P[V + r] = p2;
-        P[2 * V + r] = p3;
     }
 }
 
 // out = in - lambda TV_div(P)   (TV_method.m:26)
-__global__ void k_tv_out(const float *P, const float *in, float *out, int n1, int n2, int n3, float lam) {
-    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
-    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
-        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
-        const long m1 = r - i1 + wrap(i1 - 1, n1);
-        const long m2 = r + (wrap(i2 - 1, n2) - i2) * s2;
-        const long m3 = r + (wrap(i3 - 1, n3) - i3) * s3;
-        const float dv = P[r] + P[V + r] + P[2 * V + r] - P[m1] - P[V + m2] - P[2 * V + m3];
-        out[r] = in[r] - lam * dv;
+__global__ void k_tv_out(const float *P, const float *in, float *out, Rows g, float lam) {
+    const long V = g.V;
+    for (int row = blockIdx.x; row < g.n2 * g.n3; row += gridDim.x) {
+        const int i2 = row % g.n2, i3 = row / g.n2;
+        const long b = g.at(i2, i3), b2 = g.at(i2 == 0 ? g.n2 - 1 : i2 - 1, i3),
+                   b3 = g.at(i2, i3 == 0 ? g.n3 - 1 : i3 - 1);
+        for (int i1 = threadIdx.x; i1 < g.n1; i1 += blockDim.x) {
+            const long r = b + i1;
+            const int i1m = i1 == 0 ? g.n1 - 1 : i1 - 1;
+            const float dv = P[r] + P[V + r] + P[2 * V + r] - P[b + i1m] - P[V + b2 + i1] - P[2 * V + b3 + i1];
+            out[r] = in[r] - lam * dv;
+        }
     }
 }
 
 // err += lambda sum |TV_del(u)|   (TV_method.m:27, 71-83), FP64 accumulation
-__global__ void k_tv_err(const float *u, int n1, int n2, int n3, double lam, double *err) {
-    const long s2 = n1, s3 = (long)n1 * n2, V = s3 * n3;
+__global__ void k_tv_err(const float *u, Rows g, double lam, double *err) {
     double acc = 0.0;
-    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < V; r += (long)gridDim.x * blockDim.x) {
-        const int i1 = (int)(r % n1), i2 = (int)((r / n1) % n2), i3 = (int)(r / s3);
-        const float u0 = u[r];
-        const float d1 = u[r - i1 + wrap(i1 + 1, n1)] - u0;
-        const float d2 = u[r + (wrap(i2 + 1, n2) - i2) * s2] - u0;
-        const float d3 = u[r + (wrap(i3 + 1, n3) - i3) * s3] - u0;
-        acc += sqrt((double)d1 * d1 + (double)d2 * d2 + (double)d3 * d3);
+    for (int row = blockIdx.x; row < g.n2 * g.n3; row += gridDim.x) {
+        const int i2 = row % g.n2, i3 = row / g.n2;
+        const long b = g.at(i2, i3), b2 = g.at(i2 == g.n2 - 1 ? 0 : i2 + 1, i3),
+                   b3 = g.at(i2, i3 == g.n3 - 1 ? 0 : i3 + 1);
+        for (int i1 = threadIdx.x; i1 < g.n1; i1 += blockDim.x) {
+            const long r = b + i1;
+            const int i1p = i1 == g.n1 - 1 ? 0 : i1 + 1;
+            const float u0 = u[r];
+            const float d1 = u[b + i1p] - u0;
+            const float d2 = u[b2 + i1] - u0;
+            const float d3 = u[b3 + i1] - u0;
+            acc += sqrt((double)d1 * d1 + (double)d2 * d2 + (double)d3 * d3);
+        }
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(err, lam * acc);
@@ -167,7 +196,11 @@ __global__ void k_update(float *rec, const double *acc, long n, float step0) {
 
 int tv_prox(const TvArgs &a, cudaStream_t st) {
     const long V = (long)a.n1 * a.n2 * a.n3;
-    const int g = grid_for(V);
+    const Rows rows{a.n1, a.n2, a.n3, V};
+    // threads over i1 (whole warps, at most 256), CTAs over rows: up to 16
+    // CTAs of 128 threads per SM
+    const int bt = std::min(256, (a.n1 + 31) / 32 * 32);
+    const int g = (int)std::min<long>((long)a.n2 * a.n3, 148L * (2048 / bt));
     cudaError_t e;
     if ((e = cudaMemsetAsync(a.P, 0, sizeof(float) * 3 * V, st)) != cudaSuccess) return (int)e;
     if ((e = cudaMemsetAsync(a.Y, 0, sizeof(float) * 3 * V, st)) != cudaSuccess) return (int)e;
@@ -177,11 +210,11 @@ int tv_prox(const TvArgs &a, cudaStream_t st) {
         const double t0 = t;
         t = (1.0 + std::sqrt(1.0 + 4.0 * t0 * t0)) / 2.0;  // TV_FISTA_method.m:31
         const double m = (t0 - 1.0) / t;
-        k_tv_d<<<g, kThreads, 0, st>>>(a.fista ? a.Y : a.P, a.in, a.D, a.n1, a.n2, a.n3, (float)(1.0 / a.lambda));
-        k_tv_step<<<g, kThreads, 0, st>>>(a.P, a.Y, a.D, a.n1, a.n2, a.n3, tau, m, a.fista);
+        k_tv_d<<<g, bt, 0, st>>>(a.fista ? a.Y : a.P, a.in, a.D, rows, (float)(1.0 / a.lambda));
+        k_tv_step<<<g, bt, 0, st>>>(a.P, a.Y, a.D, rows, tau, m, a.fista);
     }
-    k_tv_out<<<g, kThreads, 0, st>>>(a.P, a.in, a.out, a.n1, a.n2, a.n3, (float)a.lambda);
-    if (a.err) k_tv_err<<<g, kThreads, 0, st>>>(a.out, a.n1, a.n2, a.n3, a.lambda, a.err);
+    k_tv_out<<<g, bt, 0, st>>>(a.P, a.in, a.out, rows, (float)a.lambda);
+    if (a.err) k_tv_err<<<g, bt, 0, st>>>(a.out, rows, a.lambda, a.err);
     return (int)cudaGetLastError();
 }
 
