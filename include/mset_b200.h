@@ -257,9 +257,10 @@ int mset_batch_read_gradient(mset_session *s, double *grad, double *probe, doubl
  * shape).  Times the batched pass on a sample of the session's own positions
  * (up to 4 x SMs x resident CTAs) for every shape whose saved-wave storage fits
  * mem_budget_bytes (0: no limit) and keeps the fastest, or among shapes within
- * 1% of it the one using less memory.  Shape = kernel thread shape (for
- * 64, 96, 128 and 160 two compiled shapes: threads per CTA and the register
- * budget that goes with them) x persistent CTAs (SMs x CTAs per
+ * 1% of it the one using less memory.  Shape = kernel thread shape (two or
+ * three compiled shapes for 64, 96, 128, 160 and 256: threads per CTA and the
+ * register budget that goes with them, row padding, or the saved waves staged
+ * by bulk copies) x persistent CTAs (SMs x CTAs per
  * SM, i.e. positions in flight) x checkpoint interval k in {0, 2, 4, 8, 16}
  * (k < slabs; k = 0 keeps every wave).  The choice stays with the session
  * (mset_batch_set_checkpoint overrides k).  MSET_E_NOMEM when no shape fits. */
@@ -275,8 +276,9 @@ typedef struct {
                                shared memory by bulk copies (TMA engine) */
 } mset_tune_result;
 int mset_batch_tune(mset_session *s, double mem_budget_bytes, mset_tune_result *out);
-/* compiled kernel shapes of window size n (threads per CTA and register
- * budget; same results), and the choice of one for a session (0: default;
+/* compiled kernel shapes of window size n that share the default shape's
+ * scrambled Fourier layout (threads per CTA, register budget, padding or
+ * staging; same results), and the choice of one for a session (0: default;
  * resets the tuned batch shape) */
 int mset_batch_variants(int n);
 int mset_batch_set_variant(mset_session *s, int variant);
